@@ -1,0 +1,950 @@
+// Host side of libafid_gpu: contexts, boxes, metric tables, batches, launch
+// sequences and the C-ABI of include/afid_gpu.h.
+#include <cmath>
+#include <cstddef>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "afid_device.cuh"
+#include "k_fft.cuh"
+#include "k_routine.cuh"
+#include "k_stencil.cuh"
+#include "../../include/afid_gpu.h"
+
+using namespace afid;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                            \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(AFID_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+#define CKL()                                                                               \
+  do {                                                                                      \
+    cudaError_t e_ = cudaGetLastError();                                                    \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(AFID_ECUDA, "launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, NFAM };
+constexpr int HIST_CAP = 4096;
+
+struct HostBox {
+  int id = -1;
+  afid_box_params prm{};
+  BoxDev dev{};           // descriptor with device pointers
+  BoxDev *d_self = nullptr;  // device copy of dev (active = 1), for single-box kernels
+  void *mem_fields = nullptr, *mem_scratch = nullptr, *mem_small = nullptr, *mem_routine = nullptr;
+  size_t scratch_doubles = 0;
+};
+
+struct Batch {
+  std::vector<int> ids;
+  BoxDev *d_boxes = nullptr;
+  int *d_off = nullptr;     // NFAM x (nbox + 1)
+  int total[NFAM] = {};
+  size_t smem_y = 0, smem_z = 0;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+};
+
+long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
+
+int factor_radices(int n, int *rad, int *np) {
+  int m = n, c = 0;
+  while (m % 4 == 0) { rad[c++] = 4; m /= 4; }
+  while (m % 2 == 0) { rad[c++] = 2; m /= 2; }
+  const int odd[3] = {3, 5, 7};
+  for (int q = 0; q < 3; ++q)
+    while (m % odd[q] == 0) { rad[c++] = odd[q]; m /= odd[q]; }
+  if (m != 1 || c > 15) return -1;
+  rad[c] = 0;
+  *np = c;
+  return 0;
+}
+
+long long tiles_of(const BoxDev &B, int fam) {
+  switch (fam) {
+    case FAM_K1: return cdiv(B.nym, K1_TJ) * cdiv(B.nzm, K1_TI);
+    case FAM_COL: return cdiv(B.plane, 256);
+    case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
+    case FAM_DIAG: return cdiv((long long)B.nxm * B.plane, 1024);
+    case FAM_FY: return (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B.nym));
+    case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B.nzm));
+    case FAM_PX: return cdiv((long long)B.nzm * B.nymh, 256);
+  }
+  return 0;
+}
+
+struct Sizes {
+  long long nx, plane, fsize, nspec, scratch, small;
+};
+
+Sizes sizes_of(const afid_box_params &p) {
+  Sizes s;
+  s.nx = p.nxm + 1;
+  s.plane = (long long)p.nym * p.nzm;
+  s.fsize = s.nx * s.plane;
+  s.nspec = (long long)p.nxm * p.nzm * (p.nym / 2 + 1);
+  long long pois = 3 * s.nspec + (long long)p.nxm * s.plane;
+  s.scratch = pois > 4 * s.fsize ? pois : 4 * s.fsize;
+  // tables + twiddles + coef + nu partials + history + scalars (in doubles)
+  s.small = (long long)T_NK * s.nx + p.nzm + p.nym + 2LL * (p.nym + p.nzm) +
+            (long long)SYS_N * C_N * s.nx + 2 * NU_BLOCKS + (long long)HIST_CAP * HIST_FIELDS +
+            (long long)(sizeof(BoxScalars) / 8 + 8) + s.plane;
+  return s;
+}
+
+// ---- metric tables: CreateGrid.F90:129-266 and InitPressureSolver.F90:22-59
+void build_tables(const afid_box_params &p, const double *xc, std::vector<double> &tab) {
+  const int nxm = p.nxm, nym = p.nym, nzm = p.nzm, nx = nxm + 1;
+  tab.assign((size_t)T_NK * nx + nzm + nym, 0.0);
+  auto T = [&](int t, int k) -> double & { return tab[(size_t)t * nx + k]; };
+  const double pi = 2.0 * std::asin(1.0);
+  const double dx = (double)nxm / p.alx3;
+  const double dxq = dx * dx;
+  std::vector<double> g3rm(nx, 0.0), g3rc(nx, 0.0);
+  for (int kc = 1; kc <= nxm; ++kc) g3rm[kc - 1] = (xc[kc] - xc[kc - 1]) * dx;
+  for (int kc = 2; kc <= nxm; ++kc) g3rc[kc - 1] = (xc[kc] - xc[kc - 2]) * dx * 0.5;
+  g3rc[0] = (xc[1] - xc[0]) * dx;
+  g3rc[nx - 1] = (xc[nx - 1] - xc[nxm - 1]) * dx;
+  for (int kc = 1; kc <= nxm; ++kc) {
+    T(T_UDX3M, kc - 1) = dx / g3rm[kc - 1];
+    T(T_UDX3C, kc - 1) = dx / g3rc[kc - 1];
+  }
+  T(T_UDX3C, nx - 1) = dx / g3rc[nx - 1];
+  // centred second derivative
+  T(T_AC3CK, 0) = 1.0; T(T_AC3CK, nx - 1) = 1.0;
+  for (int kc = 2; kc <= nxm; ++kc) {
+    const double a33 = dxq / g3rc[kc - 1];
+    const double a33p = 1.0 / g3rm[kc - 1];
+    const double a33m = 1.0 / g3rm[kc - 2];
+    T(T_AP3CK, kc - 1) = a33 * a33p;
+    T(T_AM3CK, kc - 1) = a33 * a33m;
+    T(T_AC3CK, kc - 1) = -(T(T_AP3CK, kc - 1) + T(T_AM3CK, kc - 1));
+  }
+  // staggered, with the wall conditions
+  for (int kc = 2; kc <= nxm - 1; ++kc) {
+    const double a33 = dxq / g3rm[kc - 1];
+    const double a33p = +a33 / g3rc[kc];
+    const double a33m = +a33 / g3rc[kc - 1];
+    T(T_AP3SK, kc - 1) = a33p;
+    T(T_AM3SK, kc - 1) = a33m;
+    T(T_AC3SK, kc - 1) = -(T(T_AP3SK, kc - 1) + T(T_AM3SK, kc - 1));
+  }
+  {
+    const int kc = 1;
+    const double a33 = dxq / g3rm[kc - 1];
+    const double a33p = +a33 / g3rc[kc];
+    const double a33m = +a33 / g3rc[kc - 1];
+    T(T_AP3SK, kc - 1) = a33p;
+    T(T_AM3SK, kc - 1) = 0.0;
+    T(T_AC3SK, kc - 1) = -(a33p + p.inslws * a33m * 2.0);
+  }
+  {
+    const int kc = nxm;
+    const double a33 = dxq / g3rm[kc - 1];
+    const double a33p = +a33 / g3rc[kc];
+    const double a33m = +a33 / g3rc[kc - 1];
+    T(T_AM3SK, kc - 1) = a33m;
+    T(T_AP3SK, kc - 1) = 0.0;
+    T(T_AC3SK, kc - 1) = -(a33m + p.inslwn * a33p * 2.0);
+  }
+  // temperature
+  T(T_AC3SSK, 0) = 1.0;
+  for (int kc = 2; kc <= nxm; ++kc) {
+    const double a33 = dxq / g3rc[kc - 1];
+    const double a33p = 1.0 / g3rm[kc - 1];
+    const double a33m = 1.0 / g3rm[kc - 2];
+    T(T_AP3SSK, kc - 1) = a33 * a33p;
+    T(T_AM3SSK, kc - 1) = a33 * a33m;
+    T(T_AC3SSK, kc - 1) = -(T(T_AP3SSK, kc - 1) + T(T_AM3SSK, kc - 1));
+  }
+  T(T_AC3SSK, nx - 1) = 1.0;
+  // Poisson x-coefficients (kmc(1) = 0, kpc(nxm) = 0)
+  for (int kc = 1; kc <= nxm; ++kc) {
+    const int kp = (kc == nxm) ? kc : kc + 1;
+    const double kmc = (kc == 1) ? 0.0 : 1.0;
+    const double kpc = (kc == nxm) ? 0.0 : 1.0;
+    const double a33icc = kmc * dxq / g3rc[kc - 1];
+    const double a33icp = kpc * dxq / g3rc[kp - 1];
+    const double ugmmm = 1.0 / g3rm[kc - 1];
+    T(T_AMPHK, kc - 1) = a33icc * ugmmm;
+    T(T_APPHK, kc - 1) = a33icp * ugmmm;
+    T(T_ACPHK, kc - 1) = -(T(T_AMPHK, kc - 1) + T(T_APPHK, kc - 1));
+  }
+  for (int k = 0; k < nx; ++k) { T(T_XC, k) = xc[k]; T(T_G3RC, k) = g3rc[k]; T(T_G3RM, k) = g3rm[k]; }
+  // modified wavenumbers
+  double *ak1 = &tab[(size_t)T_NK * nx];
+  double *ak2 = ak1 + nzm;
+  const int nzmh = nzm / 2 + 1, nymh = nym / 2 + 1;
+  for (int i = 1; i <= nzm; ++i) {
+    const double ao = (i <= nzmh) ? (i - 1) * 2.0 * pi : -(nzm - i + 1) * 2.0 * pi;
+    const double f = (double)nzm / p.zlen;
+    ak1[i - 1] = 2.0 * (1.0 - std::cos(ao / nzm)) * (f * f);
+  }
+  for (int j = 1; j <= nym; ++j) {
+    const double ap = (j <= nymh) ? (j - 1) * 2.0 * pi : -(nym - j + 1) * 2.0 * pi;
+    const double f = (double)nym / p.ylen;
+    ak2[j - 1] = 2.0 * (1.0 - std::cos(ap / nym)) * (f * f);
+  }
+}
+
+void build_twiddles(int n, double2 *w) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int k = 0; k < n; ++k) {
+    const long double a = 2.0L * pi * (long double)k / (long double)n;
+    w[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
+  }
+}
+
+}  // namespace
+
+struct afid_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::map<int, HostBox *> boxes;
+  int next_id = 0;
+  std::map<std::vector<int>, Batch *> batches;
+  std::vector<double> staging_host;
+};
+
+namespace {
+
+int set_device(afid_ctx *c) {
+  CK(cudaSetDevice(c->device));
+  return 0;
+}
+
+void free_batch(Batch *bt) {
+  if (!bt) return;
+  if (bt->gexec) cudaGraphExecDestroy(bt->gexec);
+  if (bt->d_boxes) cudaFree(bt->d_boxes);
+  if (bt->d_off) cudaFree(bt->d_off);
+  delete bt;
+}
+
+int get_box(afid_ctx *c, int id, HostBox **out) {
+  auto it = c->boxes.find(id);
+  if (it == c->boxes.end()) return fail(AFID_ENOBOX, "unknown box id %d", id);
+  *out = it->second;
+  return 0;
+}
+
+int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
+  if (n <= 0 || !ids) return fail(AFID_EINVAL, "empty box set");
+  std::vector<int> key(ids, ids + n);
+  auto it = c->batches.find(key);
+  if (it != c->batches.end()) { *out = it->second; return 0; }
+  std::vector<BoxDev> devs;
+  std::vector<int> off((size_t)NFAM * (n + 1), 0);
+  Batch *bt = new Batch();
+  bt->ids = key;
+  for (int b = 0; b < n; ++b) {
+    HostBox *hb;
+    int rc = get_box(c, ids[b], &hb);
+    if (rc) { delete bt; return rc; }
+    BoxDev d = hb->dev;
+    d.active = 1;
+    devs.push_back(d);
+    const size_t sy = (size_t)2 * fft_y_pairs(d.nym) * d.nym * sizeof(double2);
+    const size_t sz = (size_t)2 * fft_z_lines(d.nzm) * d.nzm * sizeof(double2);
+    if (sy > bt->smem_y) bt->smem_y = sy;
+    if (sz > bt->smem_z) bt->smem_z = sz;
+  }
+  for (int f = 0; f < NFAM; ++f) {
+    long long acc = 0;
+    for (int b = 0; b < n; ++b) {
+      off[(size_t)f * (n + 1) + b] = (int)acc;
+      acc += tiles_of(devs[b], f);
+    }
+    if (acc > 0x7fffffffLL) { delete bt; return fail(AFID_ESIZE, "grid too large"); }
+    off[(size_t)f * (n + 1) + n] = (int)acc;
+    bt->total[f] = (int)acc;
+  }
+  if (cudaMalloc(&bt->d_boxes, sizeof(BoxDev) * n) != cudaSuccess ||
+      cudaMalloc(&bt->d_off, sizeof(int) * off.size()) != cudaSuccess) {
+    free_batch(bt);
+    return fail(AFID_ENOMEM, "batch descriptor allocation failed");
+  }
+  CK(cudaMemcpy(bt->d_boxes, devs.data(), sizeof(BoxDev) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(bt->d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+  c->batches[key] = bt;
+  *out = bt;
+  return 0;
+}
+
+BatchDev bdev(const Batch *bt, int fam) {
+  BatchDev d;
+  d.boxes = bt->d_boxes;
+  d.tile_off = bt->d_off + (size_t)fam * (bt->ids.size() + 1);
+  d.nbox = (int)bt->ids.size();
+  return d;
+}
+
+int init_kernel_attrs() {
+  static bool done = false;
+  if (done) return 0;
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
+  CK(cudaFuncSetAttribute(k_fft_y_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
+  CK(cudaFuncSetAttribute(k_fft_y_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
+  CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
+  CK(cudaFuncSetAttribute(k_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
+  done = true;
+  return 0;
+}
+
+// ---- launch sequences ------------------------------------------------------
+int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel) {
+  if (from_vel)
+    k_fft_y_fwd<true><<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
+  else
+    k_fft_y_fwd<false><<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
+  CKL();
+  k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, -1);
+  CKL();
+  k_poisson_x<<<bt->total[FAM_PX], 256, 0, s>>>(bdev(bt, FAM_PX), ns);
+  CKL();
+  k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, +1);
+  CKL();
+  k_fft_y_inv<<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
+  CKL();
+  return 0;
+}
+
+int launch_substep(const Batch *bt, cudaStream_t s, int ns) {
+  const int nb = (int)bt->ids.size();
+  k_substep_prep<<<nb, 256, 0, s>>>(bt->d_boxes, nb, ns);
+  CKL();
+  k_explicit_implicit_fwd<<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
+  CKL();
+  k_implicit_bwd<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
+  CKL();
+  int rc = launch_poisson(bt, s, ns, true);
+  if (rc) return rc;
+  k_correct<<<bt->total[FAM_CELL], 256, 0, s>>>(bdev(bt, FAM_CELL), ns, 1, 1);
+  CKL();
+  return 0;
+}
+
+int launch_step(const Batch *bt, cudaStream_t s) {
+  const int nb = (int)bt->ids.size();
+  k_diag<<<bt->total[FAM_DIAG], 256, 0, s>>>(bdev(bt, FAM_DIAG));
+  CKL();
+  k_finalize<<<cdiv(nb, 128), 128, 0, s>>>(bt->d_boxes, nb, 0);
+  CKL();
+  for (int ns = 0; ns < 3; ++ns) {
+    int rc = launch_substep(bt, s, ns);
+    if (rc) return rc;
+  }
+  k_plate_nu<<<dim3(NU_BLOCKS, nb), 256, 0, s>>>(bt->d_boxes, nb);
+  CKL();
+  k_finalize<<<cdiv(nb, 128), 128, 0, s>>>(bt->d_boxes, nb, 1);
+  CKL();
+  return 0;
+}
+
+int field_ptr(HostBox *hb, int field, double **ptr, long long *rows, bool need_alloc) {
+  BoxDev &d = hb->dev;
+  *rows = d.nx;
+  switch (field) {
+    case AFID_VX: *ptr = d.vx; return 0;
+    case AFID_VY: *ptr = d.vy; return 0;
+    case AFID_VZ: *ptr = d.vz; return 0;
+    case AFID_TEMP: *ptr = d.temp; return 0;
+    case AFID_PR: *ptr = d.pr; return 0;
+    case AFID_RUX: *ptr = d.rux; return 0;
+    case AFID_RUY: *ptr = d.ruy; return 0;
+    case AFID_RUZ: *ptr = d.ruz; return 0;
+    case AFID_RUTEMP: *ptr = d.rutemp; return 0;
+    case AFID_DPH: *ptr = d.phi; *rows = d.nxm; return 0;
+    case AFID_WALL: *ptr = d.wall; *rows = 1; return 0;
+    default: break;
+  }
+  if (field >= AFID_QCAP && field <= AFID_RHS) {
+    if (!d.qcap) {
+      if (!need_alloc) return fail(AFID_EINVAL, "routine buffers not allocated");
+      return fail(AFID_EINVAL, "internal: routine buffers missing");
+    }
+    *ptr = field == AFID_QCAP ? d.qcap : field == AFID_DQ ? d.dq : field == AFID_HRO ? d.hro : d.rhs;
+    return 0;
+  }
+  return fail(AFID_EINVAL, "unknown field %d", field);
+}
+
+int sync_self(HostBox *hb) {
+  BoxDev d = hb->dev;
+  d.active = 1;
+  CK(cudaMemcpy(hb->d_self, &d, sizeof(BoxDev), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int ensure_routine_bufs(afid_ctx *c, HostBox *hb) {
+  if (hb->mem_routine) return 0;
+  const size_t fs = (size_t)hb->dev.fsize;
+  if (cudaMalloc(&hb->mem_routine, 4 * fs * sizeof(double)) != cudaSuccess)
+    return fail(AFID_ENOMEM, "routine buffers: out of device memory");
+  CK(cudaMemsetAsync(hb->mem_routine, 0, 4 * fs * sizeof(double), c->stream));
+  double *r = (double *)hb->mem_routine;
+  hb->dev.qcap = r; hb->dev.dq = r + fs; hb->dev.hro = r + 2 * fs; hb->dev.rhs = r + 3 * fs;
+  // batches hold copies of the descriptor: drop them
+  for (auto it = c->batches.begin(); it != c->batches.end();) {
+    free_batch(it->second);
+    it = c->batches.erase(it);
+  }
+  return sync_self(hb);
+}
+
+int single_batch(afid_ctx *c, int id, Batch **bt) { return get_batch(c, &id, 1, bt); }
+
+}  // namespace
+
+// ============================================================================
+// C-ABI
+// ============================================================================
+extern "C" {
+
+int afid_version(void) { return 10000; }
+
+const char *afid_last_error(void) { return g_err.c_str(); }
+
+int afid_ctx_create(afid_ctx **out, int device) {
+  if (!out) return fail(AFID_EINVAL, "null ctx pointer");
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(AFID_EINVAL, "device %d out of range (%d)", device, ndev);
+  afid_ctx *c = new afid_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(AFID_ECUDA, "ctx create: %s", cudaGetErrorString(e));
+  }
+  c->stream = c->own;
+  int rc = init_kernel_attrs();
+  if (rc) { cudaStreamDestroy(c->own); delete c; return rc; }
+  *out = c;
+  return 0;
+}
+
+int afid_ctx_destroy(afid_ctx *c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto &kv : c->batches) free_batch(kv.second);
+  for (auto &kv : c->boxes) {
+    HostBox *hb = kv.second;
+    cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small);
+    cudaFree(hb->mem_routine); cudaFree(hb->d_self);
+    delete hb;
+  }
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return 0;
+}
+
+int afid_ctx_set_stream(afid_ctx *c, void *stream) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  return 0;
+}
+
+void *afid_ctx_stream(afid_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int afid_ctx_synchronize(afid_ctx *c) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int afid_make_grid(int nxm, int istr3, double str3, double alx3, double *xc) {
+  if (nxm < 2 || !xc) return fail(AFID_EINVAL, "make_grid: nxm >= 2 and xc required");
+  const int nx = nxm + 1;
+  const double pi = 2.0 * std::asin(1.0);
+  if (istr3 == 0) {
+    for (int kc = 1; kc <= nx; ++kc) xc[kc - 1] = alx3 * ((double)(kc - 1) / (double)nxm);
+  } else if (istr3 == 4) {
+    const double tstr3 = std::tanh(str3);
+    xc[0] = 0.0;
+    for (int kc = 2; kc <= nx; ++kc) {
+      const double z2dp = (double)(2 * kc - nx - 1) / (double)nxm;
+      xc[kc - 1] = (1 + std::tanh(str3 * z2dp) / tstr3) * 0.5 * alx3;
+      if (xc[kc - 1] < 0 || xc[kc - 1] > alx3) return fail(AFID_EINVAL, "grid is too stretched");
+    }
+  } else if (istr3 == 6) {
+    const int nclip = (int)str3;
+    const int nxmo = nx + nclip + nclip;
+    std::vector<double> etaz(nx);
+    for (int kc = 1; kc <= nx; ++kc)
+      etaz[kc - 1] = std::cos(pi * ((double)(kc + nclip) - 0.5) / (double)nxmo);
+    const double delet = etaz[0] - etaz[nx - 1];
+    for (int kc = 1; kc <= nx; ++kc) etaz[kc - 1] = etaz[kc - 1] / (0.5 * delet);
+    xc[0] = 0.0;
+    for (int kc = 2; kc <= nxm; ++kc) xc[kc - 1] = alx3 * (1.0 - etaz[kc - 1]) * 0.5;
+    xc[nx - 1] = alx3;
+  } else if (istr3 == 7) {
+    for (int kc = 1; kc <= nx; ++kc)
+      xc[kc - 1] = alx3 * 0.5 * (1.0 - std::cos(pi * (double)(kc - 1) / (double)nxm));
+    xc[0] = 0.0;
+    xc[nx - 1] = alx3;
+  } else {
+    return fail(AFID_EINVAL, "istr3=%d not supported (0, 4, 6, 7)", istr3);
+  }
+  return 0;
+}
+
+size_t afid_box_device_bytes(const afid_box_params *p) {
+  if (!p) return 0;
+  Sizes s = sizes_of(*p);
+  return (size_t)(9 * s.fsize + s.scratch + s.small) * sizeof(double) + 2 * sizeof(BoxDev) + 4096;
+}
+
+int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *box_id) {
+  if (!c || !p || !xc || !box_id) return fail(AFID_EINVAL, "box_add: null argument");
+  if (p->nxm < 3 || p->nym < 2 || p->nzm < 2) return fail(AFID_EINVAL, "box_add: nxm >= 3, nym, nzm >= 2");
+  if (p->nym % 2) return fail(AFID_EINVAL, "box_add: nym must be even (real FFT along y)");
+  if (p->nym > 8192 || p->nzm > 8192) return fail(AFID_ESIZE, "box_add: nym, nzm <= 8192");
+  if (p->nsst != 1 && p->nsst != 3) return fail(AFID_EINVAL, "box_add: nsst must be 1 or 3");
+  if (!(p->ray > 0) || !(p->pra > 0) || !(p->ylen > 0) || !(p->zlen > 0) || !(p->alx3 > 0))
+    return fail(AFID_EINVAL, "box_add: ray, pra, ylen, zlen, alx3 must be > 0");
+  for (int k = 1; k <= p->nxm; ++k)
+    if (!(xc[k] > xc[k - 1])) return fail(AFID_EINVAL, "box_add: xc must be increasing");
+  int rc = set_device(c);
+  if (rc) return rc;
+  HostBox *hb = new HostBox();
+  hb->prm = *p;
+  BoxDev &d = hb->dev;
+  d.nxm = p->nxm; d.nx = p->nxm + 1; d.nym = p->nym; d.nzm = p->nzm; d.nymh = p->nym / 2 + 1;
+  d.nsst = p->nsst; d.inslws = p->inslws; d.inslwn = p->inslwn;
+  if (factor_radices(d.nym, d.fft_y_radix, &d.fft_y_np) || factor_radices(d.nzm, d.fft_z_radix, &d.fft_z_np)) {
+    delete hb;
+    return fail(AFID_EFFT, "FFT size not efficient: nym=%d nzm=%d need prime factors <= 7 (code 444)", p->nym, p->nzm);
+  }
+  Sizes s = sizes_of(*p);
+  d.plane = s.plane; d.fsize = s.fsize; d.nspec = s.nspec;
+  d.dx = (double)p->nxm / p->alx3; d.dy = (double)p->nym / p->ylen; d.dz = (double)p->nzm / p->zlen;
+  d.dxq = d.dx * d.dx; d.dyq = d.dy * d.dy; d.dzq = d.dz * d.dz;
+  d.ren = std::sqrt(p->ray / p->pra);
+  d.pec = std::sqrt(p->pra * p->ray);
+  d.tempbp = p->tempbp; d.temptp = p->temptp;
+  d.hist_cap = HIST_CAP;
+  const size_t fb = 9 * (size_t)s.fsize * sizeof(double);
+  const size_t sb = (size_t)s.scratch * sizeof(double);
+  const size_t mb = (size_t)s.small * sizeof(double);
+  if (cudaMalloc(&hb->mem_fields, fb) != cudaSuccess || cudaMalloc(&hb->mem_scratch, sb) != cudaSuccess ||
+      cudaMalloc(&hb->mem_small, mb) != cudaSuccess || cudaMalloc(&hb->d_self, sizeof(BoxDev)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small); cudaFree(hb->d_self);
+    delete hb;
+    return fail(AFID_ENOMEM, "box_add: out of device memory (%zu bytes)", fb + sb + mb);
+  }
+  double *F = (double *)hb->mem_fields;
+  d.vx = F; d.vy = F + s.fsize; d.vz = F + 2 * s.fsize; d.temp = F + 3 * s.fsize; d.pr = F + 4 * s.fsize;
+  d.rux = F + 5 * s.fsize; d.ruy = F + 6 * s.fsize; d.ruz = F + 7 * s.fsize; d.rutemp = F + 8 * s.fsize;
+  double *Sc = (double *)hb->mem_scratch;
+  for (int q = 0; q < 4; ++q) d.ybuf[q] = Sc + q * s.fsize;
+  d.spec = (double2 *)Sc;
+  d.dstore = Sc + 2 * s.nspec;
+  d.phi = Sc + 3 * s.nspec;
+  hb->scratch_doubles = (size_t)s.scratch;
+  // small allocations
+  double *M = (double *)hb->mem_small;
+  size_t o = 0;
+  std::vector<double> tab;
+  build_tables(*p, xc, tab);
+  d.tab = M + o; o += tab.size();
+  o = (o + 1) & ~(size_t)1;
+  d.twy = (const double2 *)(M + o); o += 2 * (size_t)p->nym;
+  d.twz = (const double2 *)(M + o); o += 2 * (size_t)p->nzm;
+  d.coef = M + o; o += (size_t)SYS_N * C_N * d.nx;
+  d.nu_part = M + o; o += 2 * NU_BLOCKS;
+  d.hist = M + o; o += (size_t)HIST_CAP * HIST_FIELDS;
+  d.wall = M + o; o += (size_t)s.plane;
+  o = (o + 7) & ~(size_t)7;
+  d.sc = (BoxScalars *)(M + o);
+  std::vector<double2> tw((size_t)p->nym + p->nzm);
+  build_twiddles(p->nym, tw.data());
+  build_twiddles(p->nzm, tw.data() + p->nym);
+  BoxScalars bs;
+  memset(&bs, 0, sizeof bs);
+  bs.dt = p->dt; bs.idtv = p->idtv; bs.cflmax = p->cflmax; bs.dtmin = p->dtmin; bs.dtmax = p->dtmax;
+  bs.limitvel = p->vlim; bs.resid = p->resid;
+  cudaStream_t st = c->stream;
+  bool ok = cudaMemsetAsync(hb->mem_fields, 0, fb, st) == cudaSuccess &&
+            cudaMemsetAsync(hb->mem_scratch, 0, sb, st) == cudaSuccess &&
+            cudaMemsetAsync(hb->mem_small, 0, mb, st) == cudaSuccess &&
+            cudaMemcpyAsync((void *)d.tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync((void *)d.twy, tw.data(), tw.size() * 16, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaStreamSynchronize(st) == cudaSuccess;
+  if (!ok) {
+    cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small); cudaFree(hb->d_self);
+    delete hb;
+    return fail(AFID_ECUDA, "box_add: initialisation copy failed");
+  }
+  hb->id = c->next_id++;
+  rc = sync_self(hb);
+  if (rc) return rc;
+  c->boxes[hb->id] = hb;
+  *box_id = hb->id;
+  return 0;
+}
+
+int afid_box_remove(afid_ctx *c, int id) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto it = c->batches.begin(); it != c->batches.end();) {
+    bool has = false;
+    for (int x : it->first) has |= (x == id);
+    if (has) { free_batch(it->second); it = c->batches.erase(it); }
+    else ++it;
+  }
+  cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small);
+  cudaFree(hb->mem_routine); cudaFree(hb->d_self);
+  c->boxes.erase(id);
+  delete hb;
+  return 0;
+}
+
+static int transfer(afid_ctx *c, int id, int field, double *host, bool up) {
+  if (!c || !host) return fail(AFID_EINVAL, "null argument");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  if (field >= AFID_QCAP && field <= AFID_RHS) {
+    rc = ensure_routine_bufs(c, hb);
+    if (rc) return rc;
+  }
+  double *dp;
+  long long rows;
+  rc = field_ptr(hb, field, &dp, &rows, true);
+  if (rc) return rc;
+  const BoxDev &d = hb->dev;
+  cudaStream_t st = c->stream;
+  if (field == AFID_WALL) {
+    const size_t bytes = (size_t)d.plane * sizeof(double);
+    if (up) CK(cudaMemcpyAsync(dp, host, bytes, cudaMemcpyHostToDevice, st));
+    else CK(cudaMemcpyAsync(host, dp, bytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
+  }
+  const size_t n = (size_t)rows * d.plane;
+  // staging: the first scratch field (the forward-sweep buffer of vx), which
+  // never overlaps dph
+  double *stg = d.ybuf[0];
+  if (field == AFID_DPH) stg = d.ybuf[0];
+  dim3 blk(32, 8);
+  dim3 grd((unsigned)cdiv(rows, 32), (unsigned)cdiv(d.nym, 32), (unsigned)d.nzm);
+  if (up) {
+    CK(cudaMemcpyAsync(stg, host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_fortran_to_dev<<<grd, blk, 0, st>>>(stg, dp, (int)rows, d.nym, d.nzm, (int)rows);
+    CKL();
+  } else {
+    k_dev_to_fortran<<<grd, blk, 0, st>>>(dp, stg, (int)rows, d.nym, d.nzm, (int)rows);
+    CKL();
+    CK(cudaMemcpyAsync(host, stg, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int afid_box_upload(afid_ctx *c, int id, int field, const double *host) {
+  return transfer(c, id, field, const_cast<double *>(host), true);
+}
+
+int afid_box_download(afid_ctx *c, int id, int field, double *host) {
+  return transfer(c, id, field, host, false);
+}
+
+int afid_box_reset(afid_ctx *c, int id, double dt) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  const BoxDev &d = hb->dev;
+  cudaStream_t st = c->stream;
+  CK(cudaMemsetAsync(d.rux, 0, 4 * (size_t)d.fsize * sizeof(double), st));
+  CK(cudaMemsetAsync(d.wall, 0, (size_t)d.plane * sizeof(double), st));
+  BoxScalars bs;
+  CK(cudaMemcpyAsync(&bs, d.sc, sizeof bs, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  bs.time = 0.0; bs.ntime = 0; bs.status = 0; bs.nonfinite = 0;
+  for (int q = 0; q < 4; ++q) bs.red_u64[q] = 0;
+  if (dt > 0) bs.dt = dt;
+  CK(cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int afid_box_get_scalars(afid_ctx *c, int id, afid_box_scalars *out) {
+  if (!c || !out) return fail(AFID_EINVAL, "null argument");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  BoxScalars bs;
+  CK(cudaMemcpyAsync(&bs, hb->dev.sc, sizeof bs, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  out->dt = bs.dt; out->time = bs.time; out->cfl = bs.cfl; out->cfl_used = bs.cfl_used;
+  out->divmax = bs.divmax;
+  for (int q = 0; q < 3; ++q) out->vmax[q] = bs.vmax[q];
+  out->nu_bot = bs.nu_bot; out->nu_top = bs.nu_top; out->ntime = bs.ntime; out->status = bs.status;
+  return 0;
+}
+
+int afid_box_history(afid_ctx *c, int id, afid_step_record *out, int max_records) {
+  if (!c || !out || max_records < 0) return fail(AFID_EINVAL, "bad argument");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  BoxScalars bs;
+  CK(cudaMemcpyAsync(&bs, hb->dev.sc, sizeof bs, cudaMemcpyDeviceToHost, c->stream));
+  std::vector<double> h((size_t)HIST_CAP * HIST_FIELDS);
+  CK(cudaMemcpyAsync(h.data(), hb->dev.hist, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int avail = bs.ntime < HIST_CAP ? bs.ntime : HIST_CAP;
+  int n = avail < max_records ? avail : max_records;
+  for (int r = 0; r < n; ++r) {
+    const int step = bs.ntime - n + r;               // 0-based step index
+    const double *src = &h[(size_t)(step % HIST_CAP) * HIST_FIELDS];
+    out[r].time = src[0]; out[r].dt = src[1]; out[r].cfl_used = src[2]; out[r].divmax = src[3];
+    out[r].nu_bot = src[4]; out[r].nu_top = src[5]; out[r].vmax_y = src[6]; out[r].vmax_z = src[7];
+  }
+  return n;
+}
+
+// ---- routine-level entry points -------------------------------------------
+int afid_time_marcher_begin_substep(afid_ctx *c, int id, int ns) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  if (ns < 0 || ns >= hb->prm.nsst) return fail(AFID_EINVAL, "substep %d out of range", ns);
+  rc = set_device(c);
+  if (rc) return rc;
+  k_substep_prep<<<1, 256, 0, c->stream>>>(hb->d_self, 1, ns);
+  CKL();
+  return 0;
+}
+
+static int explicit_one(afid_ctx *c, int id, int field) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  rc = ensure_routine_bufs(c, hb);
+  if (rc) return rc;
+  const BoxDev &d = hb->dev;
+  k_explicit_one<<<(unsigned)cdiv((long long)d.nxm * d.plane, 256), 256, 0, c->stream>>>(hb->d_self, field);
+  CKL();
+  return 0;
+}
+
+static int implicit_one(afid_ctx *c, int id, int field) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  rc = ensure_routine_bufs(c, hb);
+  if (rc) return rc;
+  const BoxDev &d = hb->dev;
+  k_implicit_one<<<(unsigned)cdiv(d.plane, 256), 256, 0, c->stream>>>(hb->d_self, field);
+  CKL();
+  return 0;
+}
+
+int afid_explicit_terms_vx(afid_ctx *c, int id) { return explicit_one(c, id, F_VX); }
+int afid_explicit_terms_vy(afid_ctx *c, int id) { return explicit_one(c, id, F_VY); }
+int afid_explicit_terms_vz(afid_ctx *c, int id) { return explicit_one(c, id, F_VZ); }
+int afid_explicit_terms_temp(afid_ctx *c, int id) { return explicit_one(c, id, F_T); }
+int afid_implicit_and_update_vx(afid_ctx *c, int id) { return implicit_one(c, id, F_VX); }
+int afid_implicit_and_update_vy(afid_ctx *c, int id) { return implicit_one(c, id, F_VY); }
+int afid_implicit_and_update_vz(afid_ctx *c, int id) { return implicit_one(c, id, F_VZ); }
+int afid_implicit_and_update_temp(afid_ctx *c, int id) { return implicit_one(c, id, F_T); }
+
+int afid_calc_local_divergence(afid_ctx *c, int id) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = single_batch(c, id, &bt);
+  if (rc) return rc;
+  k_divergence<<<bt->total[FAM_CELL], 256, 0, c->stream>>>(bdev(bt, FAM_CELL));
+  CKL();
+  return 0;
+}
+
+int afid_solve_pressure_correction(afid_ctx *c, int id) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = single_batch(c, id, &bt);
+  if (rc) return rc;
+  return launch_poisson(bt, c->stream, 0, false);
+}
+
+static int correct(afid_ctx *c, int id, int vel, int pr) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = single_batch(c, id, &bt);
+  if (rc) return rc;
+  k_correct<<<bt->total[FAM_CELL], 256, 0, c->stream>>>(bdev(bt, FAM_CELL), 0, vel, pr);
+  CKL();
+  return 0;
+}
+
+int afid_correct_velocity(afid_ctx *c, int id) { return correct(c, id, 1, 0); }
+int afid_correct_pressure(afid_ctx *c, int id) { return correct(c, id, 0, 1); }
+
+static int diag_now(afid_ctx *c, int id, BoxScalars *bs) {
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = single_batch(c, id, &bt);
+  if (rc) return rc;
+  HostBox *hb;
+  rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  void *red = (char *)hb->dev.sc + offsetof(BoxScalars, red_u64);
+  CK(cudaMemsetAsync(red, 0, sizeof(bs->red_u64), c->stream));
+  k_diag<<<bt->total[FAM_DIAG], 256, 0, c->stream>>>(bdev(bt, FAM_DIAG));
+  CKL();
+  CK(cudaMemcpyAsync(bs, hb->dev.sc, sizeof(BoxScalars), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(red, 0, sizeof(bs->red_u64), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int afid_calc_max_cfl(afid_ctx *c, int id, double *cflm) {
+  if (!c || !cflm) return fail(AFID_EINVAL, "null argument");
+  BoxScalars bs;
+  int rc = diag_now(c, id, &bs);
+  if (rc) return rc;
+  double v;
+  long long bits = (long long)bs.red_u64[0];
+  memcpy(&v, &bits, 8);
+  *cflm = v > 0.00000001 ? v : 0.00000001;
+  return 0;
+}
+
+int afid_check_divergence(afid_ctx *c, int id, double *qmax) {
+  if (!c || !qmax) return fail(AFID_EINVAL, "null argument");
+  BoxScalars bs;
+  int rc = diag_now(c, id, &bs);
+  if (rc) return rc;
+  long long bits = (long long)bs.red_u64[1];
+  memcpy(qmax, &bits, 8);
+  return 0;
+}
+
+int afid_calc_plate_nu(afid_ctx *c, int id, double *nuslow, double *nusupp) {
+  if (!c || !nuslow || !nusupp) return fail(AFID_EINVAL, "null argument");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  k_plate_nu<<<dim3(NU_BLOCKS, 1), 256, 0, c->stream>>>(hb->d_self, 1);
+  CKL();
+  double part[2 * NU_BLOCKS];
+  CK(cudaMemcpyAsync(part, hb->dev.nu_part, sizeof part, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double lo = 0.0, up = 0.0;
+  for (int q = 0; q < NU_BLOCKS; ++q) { lo += part[2 * q]; up += part[2 * q + 1]; }
+  *nuslow = lo / (double)(hb->dev.nzm * hb->dev.nym);
+  *nusupp = up / (double)(hb->dev.nzm * hb->dev.nym);
+  return 0;
+}
+
+// ---- fused path ---------------------------------------------------------------
+int afid_substep(afid_ctx *c, const int *ids, int n, int ns) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  if (ns < 0 || ns > 2) return fail(AFID_EINVAL, "substep %d out of range", ns);
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  return launch_substep(bt, c->stream, ns);
+}
+
+int afid_step(afid_ctx *c, const int *ids, int n, int nsteps) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  if (nsteps < 0) return fail(AFID_EINVAL, "nsteps < 0");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; ++s) {
+    rc = launch_step(bt, c->stream);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int afid_step_graph(afid_ctx *c, const int *ids, int n, int nsteps) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  if (nsteps < 0) return fail(AFID_EINVAL, "nsteps < 0");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  if (!bt->gexec || bt->gstream != c->stream) {
+    if (bt->gexec) { cudaGraphExecDestroy(bt->gexec); bt->gexec = nullptr; }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    rc = launch_step(bt, c->stream);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(AFID_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&bt->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { bt->gexec = nullptr; return fail(AFID_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    bt->gstream = c->stream;
+  }
+  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(bt->gexec, c->stream));
+  return 0;
+}
+
+}  // extern "C"

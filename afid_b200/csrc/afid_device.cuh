@@ -1,0 +1,138 @@
+// Device-side data structures shared by every kernel of the AFiD RK3 path.
+//
+// Field layout in HBM ("plane-major"): a 3-D field q(k, j, i) of the
+// reference (x = wall-normal k, periodic y = j, periodic z = i; Fortran
+// order k fastest) is stored as q[k][i][j], i.e. y fastest, then z, then x.
+//   * the x-tridiagonal solves run one thread per (j, i) column and march k,
+//     so a warp reads 32 consecutive j: coalesced;
+//   * the y-FFT reads contiguous y-rows;
+//   * the z-FFT reads tiles of consecutive ky for every kz;
+//   * the explicit stencils march k with a (y, z) tile in shared memory and
+//     keep the x-neighbours of their own column in a ring of planes.
+// There is no halo storage: periodic neighbours are index wraps.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace afid {
+
+// Per-box scalars that live on the device so that dt can be chosen on the
+// device (CFL rule) and a whole step can be captured in a CUDA graph.
+struct BoxScalars {
+  double dt;        // current time step
+  double time;      // simulation time
+  double al, ga, ro, beta;   // current substep coefficients, beta = dt/(2 Re)
+  double cfl;       // max CFL number of the current velocity (CalcMaxCFL)
+  double cfl_used;  // cfl*dt (fixed dt) or cfl (variable dt), main.F90:171-189
+  double divmax;    // max |div u| (CheckDivergence, without 1/(al dt))
+  double vmax[3];   // max |vz|, |vy|, |vx| (GlobalQuantities vmax order)
+  double nu_bot, nu_top;     // plate Nusselt numbers (CalcPlateNu)
+  // dt policy (bou.in)
+  double cflmax, dtmin, dtmax, limitvel, resid;
+  int idtv;         // 1 = variable dt
+  int ntime;        // step counter (main.F90 ntime)
+  int status;       // 0 ok, else the reference's error code (165/166/169/266)
+  int nonfinite;    // set when a non-finite value is seen by the diagnostics
+  unsigned long long red_u64[4];  // atomicMax scratch: cfl, div, vmax_y, vmax_z
+  double nu_partial_dummy;
+};
+
+// Offsets of the metric tables inside BoxDev::tab (length nx each unless
+// noted).  Index k is 0-based (k = kc-1 of the reference).
+enum TabId {
+  T_UDX3C = 0, T_UDX3M, T_AM3CK, T_AC3CK, T_AP3CK, T_AM3SK, T_AC3SK, T_AP3SK,
+  T_AM3SSK, T_AC3SSK, T_AP3SSK, T_AMPHK, T_ACPHK, T_APPHK, T_XC, T_G3RC,
+  T_G3RM, T_NK  // number of k-tables
+};
+
+// Per-substep tridiagonal tables in BoxDev::coef: for system s in
+// {SYS_X (vx, size nx), SYS_YZ (vy/vz, size nxm), SYS_T (temp, size nx)}
+// the arrays (sc, fact, dp, du, g) each of length nx at
+// coef[(s * C_N + a) * nx + k].
+enum SysId { SYS_X = 0, SYS_YZ = 1, SYS_T = 2, SYS_N = 3 };
+enum CoefId { C_SC = 0, C_FACT, C_DP, C_DU, C_G, C_N };
+
+constexpr int HIST_FIELDS = 8;   // time, dt, cfl_used, divmax, nu_bot, nu_top, vmax_y, vmax_z
+
+struct BoxDev {
+  int nx, nxm, nym, nzm, nymh;
+  int nsst;
+  int inslws, inslwn;
+  long long plane;      // nym * nzm
+  long long fsize;      // nx * plane
+  long long nspec;      // nxm * nzm * nymh
+  double dx, dy, dz, dxq, dyq, dzq, ren, pec, tempbp, temptp;
+  double inv_nyz;       // unused by kernels; kept for diagnostics
+  // prognostic fields, nx planes each
+  double *vx, *vy, *vz, *temp, *pr;
+  // RK history (H of the previous substep)
+  double *rux, *ruy, *ruz, *rutemp;
+  // the reference's rhs(1, :, :) row, carried between implicit solves
+  double *wall;
+  // forward-sweep intermediates of the four implicit solves (scratch)
+  double *ybuf[4];
+  // Poisson scratch (aliases ybuf storage; live only between the divergence
+  // and the correction)
+  double2 *spec;        // [k][kz][ky], k < nxm, ky <= nym/2
+  double *dstore;       // Thomas pivots of the Poisson solve, same indexing
+  double *phi;          // pressure correction dph, [k][i][j], k < nxm
+  // reference-boundary mode buffers (allocated on first use)
+  double *qcap, *dq, *hro, *rhs;
+  // tables
+  const double *tab;    // T_NK*nx k-tables, then ak1[nzm], ak2[nym]
+  const double2 *twy;   // exp(-2 pi i n / nym), n < nym
+  const double2 *twz;   // exp(-2 pi i n / nzm), n < nzm
+  double *coef;         // per-substep tridiagonal tables
+  double *nu_part;      // per-block partial sums of the plate Nu reduction
+  double *hist;         // per-step records, HIST_FIELDS doubles each (ring)
+  int hist_cap;
+  int pad1_;
+  BoxScalars *sc;
+  int fft_y_radix[16];  // radices of nym (Stockham passes), terminated by 0
+  int fft_z_radix[16];  // radices of nzm
+  int fft_y_np, fft_z_np;
+  int active;           // 0 = skipped by every kernel
+  int pad_;
+};
+
+// Work decomposition: each kernel family launches a 1-D grid over the
+// concatenated tiles of all boxes of a batch.  tile_off[b] is the first
+// block of box b, tile_off[nbox] the total.
+struct BatchDev {
+  const BoxDev *boxes;
+  const int *tile_off;  // [nbox + 1] for this kernel family
+  int nbox;
+};
+
+__device__ __forceinline__ int find_box(const int *off, int nbox, int blk) {
+  int lo = 0, hi = nbox - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= blk) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ double tabk(const BoxDev &B, int t, int k) {
+  return __ldg(B.tab + (long long)t * B.nx + k);
+}
+
+__device__ __forceinline__ int wrap(int a, int n) {
+  return a < 0 ? a + n : (a >= n ? a - n : a);
+}
+
+// Complex helpers (double2 = re, im).
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// Order-preserving map of a non-negative double onto uint64 for atomicMax.
+__device__ __forceinline__ unsigned long long dbits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+
+}  // namespace afid

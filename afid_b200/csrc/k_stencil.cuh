@@ -1,0 +1,690 @@
+// Explicit advection/diffusion terms, Crank-Nicolson right-hand sides and the
+// x-direction tridiagonal solves of one RK3 substep, plus the projection
+// (CorrectVelocity + CorrectPressure) and the per-step reductions.
+//
+// Arithmetic follows the reference expression by expression; the library is
+// compiled without FMA contraction so that every stencil value is the same
+// IEEE result the reference's x86-64 build computes for the same inputs.
+#pragma once
+#include "afid_device.cuh"
+
+namespace afid {
+
+enum FieldId { F_VX = 0, F_VY = 1, F_VZ = 2, F_T = 3, F_PR = 4, F_NF = 5 };
+
+struct StencilConst {
+  double udy, udz;           // dy/4, dz/4
+  double udyq_re, udzq_re;   // dyq/ren, dzq/ren
+  double udyq_pe, udzq_pe;   // dyq/pec, dzq/pec
+};
+
+__device__ __forceinline__ StencilConst make_sconst(const BoxDev &B) {
+  StencilConst c;
+  c.udy = B.dy * 0.25;
+  c.udz = B.dz * 0.25;
+  c.udyq_re = B.dyq / B.ren;
+  c.udzq_re = B.dzq / B.ren;
+  c.udyq_pe = B.dyq / B.pec;
+  c.udzq_pe = B.dzq / B.pec;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// The four explicit terms.  ``a(f, dk, dj, di)`` returns field f at
+// (k+dk, j+dj, i+di) around the point being computed; dk is -1, 0 or +1.
+// ``dkm``/``dkp`` are kmv(kc)-kc and kpv(kc)-kc (0 at the walls).
+// ---------------------------------------------------------------------------
+// ExplicitTermsVX.F90:55-101 (k = 2..nxm)
+template <class A>
+__device__ __forceinline__ double h_vx(const A &a, const StencilConst &c, double udx3c_k) {
+  const double vxc = a(F_VX, 0, 0, 0);
+  double hxz = (((a(F_VZ, 0, 0, 1) + a(F_VZ, -1, 0, 1)) * (a(F_VX, 0, 0, 1) + vxc))
+                - ((a(F_VZ, 0, 0, 0) + a(F_VZ, -1, 0, 0)) * (vxc + a(F_VX, 0, 0, -1)))) * c.udz;
+  double hxy = (((a(F_VY, 0, 1, 0) + a(F_VY, -1, 1, 0)) * (a(F_VX, 0, 1, 0) + vxc))
+                - ((a(F_VY, 0, 0, 0) + a(F_VY, -1, 0, 0)) * (vxc + a(F_VX, 0, -1, 0)))) * c.udy;
+  const double p = a(F_VX, 1, 0, 0) + vxc;
+  const double m = vxc + a(F_VX, -1, 0, 0);
+  double hxx = (p * p - m * m) * udx3c_k * 0.25;
+  double tempit = a(F_T, 0, 0, 0);
+  double dzzvx = (a(F_VX, 0, 0, -1) - 2.0 * vxc + a(F_VX, 0, 0, 1)) * c.udzq_re;
+  double dyyvx = (a(F_VX, 0, -1, 0) - 2.0 * vxc + a(F_VX, 0, 1, 0)) * c.udyq_re;
+  return -(hxx + hxy + hxz) + dyyvx + dzzvx + tempit;
+}
+
+// ExplicitTermsVY.F90:54-98 (k = 1..nxm)
+template <class A>
+__device__ __forceinline__ double h_vy(const A &a, const StencilConst &c, double udx3m_k, int dkm, int dkp) {
+  const double vyc = a(F_VY, 0, 0, 0);
+  double hyx = ((a(F_VX, 1, 0, 0) + a(F_VX, 1, -1, 0)) * (a(F_VY, dkp, 0, 0) + vyc)
+                - (a(F_VX, 0, 0, 0) + a(F_VX, 0, -1, 0)) * (vyc + a(F_VY, dkm, 0, 0))) * udx3m_k * 0.25;
+  const double p = a(F_VY, 0, 1, 0) + vyc;
+  const double m = a(F_VY, 0, -1, 0) + vyc;
+  double hyy = (p * p - m * m) * c.udy;
+  double hyz = ((a(F_VY, 0, 0, 1) + vyc) * (a(F_VZ, 0, 0, 1) + a(F_VZ, 0, -1, 1))
+                - (vyc + a(F_VY, 0, 0, -1)) * (a(F_VZ, 0, 0, 0) + a(F_VZ, 0, -1, 0))) * c.udz;
+  double dyyvy = (a(F_VY, 0, 1, 0) - 2.0 * vyc + a(F_VY, 0, -1, 0)) * c.udyq_re;
+  double dzzvy = (a(F_VY, 0, 0, 1) - 2.0 * vyc + a(F_VY, 0, 0, -1)) * c.udzq_re;
+  return -(hyx + hyy + hyz) + dyyvy + dzzvy;
+}
+
+// ExplicitTermsVZ.F90:56-101 (k = 1..nxm)
+template <class A>
+__device__ __forceinline__ double h_vz(const A &a, const StencilConst &c, double udx3m_k, int dkm, int dkp) {
+  const double vzc = a(F_VZ, 0, 0, 0);
+  const double p = a(F_VZ, 0, 0, 1) + vzc;
+  const double m = a(F_VZ, 0, 0, -1) + vzc;
+  double hzz = (p * p - m * m) * c.udz;
+  double hzy = ((a(F_VY, 0, 1, 0) + a(F_VY, 0, 1, -1)) * (a(F_VZ, 0, 1, 0) + vzc)
+                - (a(F_VY, 0, 0, 0) + a(F_VY, 0, 0, -1)) * (vzc + a(F_VZ, 0, -1, 0))) * c.udy;
+  double hzx = ((a(F_VX, 1, 0, 0) + a(F_VX, 1, 0, -1)) * (a(F_VZ, dkp, 0, 0) + vzc)
+                - (a(F_VX, 0, 0, 0) + a(F_VX, 0, 0, -1)) * (vzc + a(F_VZ, dkm, 0, 0))) * udx3m_k * 0.25;
+  double dzzvz = (a(F_VZ, 0, 0, 1) - 2.0 * vzc + a(F_VZ, 0, 0, -1)) * c.udzq_re;
+  double dyyvz = (a(F_VZ, 0, 1, 0) - 2.0 * vzc + a(F_VZ, 0, -1, 0)) * c.udyq_re;
+  return -(hzx + hzy + hzz) + dyyvz + dzzvz;
+}
+
+// ExplicitTermsTemp.F90:52-93 (k = 2..nxm)
+template <class A>
+__device__ __forceinline__ double h_temp(const A &a, const StencilConst &c, double udx3c_k) {
+  const double tc = a(F_T, 0, 0, 0);
+  double htz = ((a(F_VZ, -1, 0, 1) + a(F_VZ, 0, 0, 1)) * (a(F_T, 0, 0, 1) + tc)
+                - (a(F_VZ, -1, 0, 0) + a(F_VZ, 0, 0, 0)) * (tc + a(F_T, 0, 0, -1))) * c.udz;
+  double hty = ((a(F_VY, 0, 1, 0) + a(F_VY, -1, 1, 0)) * (a(F_T, 0, 1, 0) + tc)
+                - (a(F_VY, 0, 0, 0) + a(F_VY, -1, 0, 0)) * (tc + a(F_T, 0, -1, 0))) * c.udy;
+  double htx = ((a(F_VX, 1, 0, 0) + a(F_VX, 0, 0, 0)) * (a(F_T, 1, 0, 0) + tc)
+                - (a(F_VX, 0, 0, 0) + a(F_VX, -1, 0, 0)) * (tc + a(F_T, -1, 0, 0))) * udx3c_k * 0.25;
+  double dzzt = (a(F_T, 0, 0, 1) - 2.0 * tc + a(F_T, 0, 0, -1)) * c.udzq_pe;
+  double dyyt = (a(F_T, 0, 1, 0) - 2.0 * tc + a(F_T, 0, -1, 0)) * c.udyq_pe;
+  return -(htx + hty + htz) + dyyt + dzzt;
+}
+
+// Implicit right-hand sides (ImplicitAndUpdate*.F90).  Returned value is the
+// unscaled rhs; the caller multiplies by the row scale of the solver.
+// ImplicitAndUpdateVX.F90:40-58
+__device__ __forceinline__ double rhs_vx(double H, double Hold, double vxp, double vxc, double vxm,
+                                         double prc, double prm, double am, double ac, double ap,
+                                         double al, double ga, double ro, double alre, double dt,
+                                         double udx3c_k) {
+  const double udx3 = al * udx3c_k;
+  const double dxx = vxp * ap + vxc * ac + vxm * am;
+  const double dxp = (prc - prm) * udx3;
+  return (ga * H + ro * Hold + alre * dxx - dxp) * dt;
+}
+// ImplicitAndUpdateVY.F90:52-63 / ImplicitAndUpdateVZ.F90:48-59; ``dp`` is
+// the pressure-gradient term already formed by the caller.
+__device__ __forceinline__ double rhs_vyz(double H, double Hold, double qp, double qc, double qm,
+                                          double am, double ac, double ap, double dp,
+                                          double ga, double ro, double alre, double dt) {
+  const double dxx = qp * ap + qc * ac + qm * am;
+  return (ga * H + ro * Hold + alre * dxx - dp) * dt;
+}
+// ImplicitAndUpdateTemp.F90:41-49
+__device__ __forceinline__ double rhs_temp(double H, double Hold, double tp, double tc, double tm,
+                                           double am, double ac, double ap,
+                                           double ga, double ro, double alpec, double dt) {
+  const double dxx = tp * ap + tc * ac + tm * am;
+  return (ga * H + ro * Hold + alpec * dxx) * dt;
+}
+
+__device__ __forceinline__ const double *coefp(const BoxDev &B, int sys, int arr) {
+  return B.coef + (long long)(sys * C_N + arr) * B.nx;
+}
+
+// ---------------------------------------------------------------------------
+// Per-substep preparation: coefficients al/ga/ro/beta and the LU factors of
+// the three x-tridiagonal matrices (SolveImpEqnUpdate_X.F90:25-44,
+// SolveImpEqnUpdate_YZ.F90:25-38, SolveImpEqnUpdate_Temp.F90:25-47), in the
+// dgttrf operation order without pivoting (the matrices are diagonally
+// dominant; a pivot that LAPACK would take is reported as status -2).
+// One block per box.
+// ---------------------------------------------------------------------------
+__global__ void k_substep_prep(const BoxDev *__restrict__ boxes, int nbox, int ns) {
+  const int b = blockIdx.x;
+  if (b >= nbox) return;
+  const BoxDev &B = boxes[b];
+  if (!B.active || ns >= B.nsst) return;
+  BoxScalars *S = B.sc;
+  if (S->status != 0) return;
+  __shared__ double s_al, s_beta, s_bx[3];
+  if (threadIdx.x == 0) {
+    double gam[3], rom[3];
+    if (B.nsst > 1) {
+      gam[0] = 8.0 / 15.0; gam[1] = 5.0 / 12.0; gam[2] = 3.0 / 4.0;
+      rom[0] = 0.0; rom[1] = -17.0 / 60.0; rom[2] = -5.0 / 12.0;
+    } else {
+      gam[0] = 1.5; gam[1] = 0.0; gam[2] = 0.0;
+      rom[0] = -0.5; rom[1] = 0.0; rom[2] = 0.0;
+    }
+    const double dt = S->dt;
+    const double al = gam[ns] + rom[ns];
+    const double beta = dt / B.ren * 0.5;     // TimeMarcher.F90:22
+    S->al = al; S->ga = gam[ns]; S->ro = rom[ns]; S->beta = beta;
+    s_al = al; s_beta = beta;
+    s_bx[SYS_X] = beta * al;
+    s_bx[SYS_YZ] = beta * al;
+    s_bx[SYS_T] = 0.5 * al * dt / B.pec;     // SolveImpEqnUpdate_Temp.F90:25
+  }
+  __syncthreads();
+  const int nx = B.nx, nxm = B.nxm;
+  // row scale, sub- and super-diagonal (stored temporarily in C_FACT / C_DU)
+  for (int t = threadIdx.x; t < 3 * nx; t += blockDim.x) {
+    const int sys = t / nx, k = t % nx;
+    double *sc = B.coef + (long long)(sys * C_N + C_SC) * nx;
+    double *dl = B.coef + (long long)(sys * C_N + C_FACT) * nx;
+    double *du = B.coef + (long long)(sys * C_N + C_DU) * nx;
+    const double bx = s_bx[sys];
+    double s = 1.0, am = 0.0, ap = 0.0;
+    if (sys == SYS_X) {
+      if (k >= 1 && k <= nxm - 1) {
+        s = 1.0 / (1.0 - tabk(B, T_AC3CK, k) * bx);
+        am = -tabk(B, T_AM3SSK, k) * bx * s;
+        ap = -tabk(B, T_AP3SSK, k) * bx * s;
+      }
+    } else if (sys == SYS_YZ) {
+      if (k <= nxm - 1) {
+        s = 1.0 / (1.0 - tabk(B, T_AC3SK, k) * bx);
+        am = -tabk(B, T_AM3SK, k) * bx * s;
+        ap = -tabk(B, T_AP3SK, k) * bx * s;
+      }
+    } else {
+      if (k >= 1 && k <= nxm - 1) {
+        s = 1.0 / (1.0 - tabk(B, T_AC3SSK, k) * bx);
+        am = -tabk(B, T_AM3SSK, k) * bx * s;
+        ap = -tabk(B, T_AP3SSK, k) * bx * s;
+      }
+    }
+    sc[k] = s; dl[k] = am; du[k] = ap;
+  }
+  __syncthreads();
+  // sequential LU recurrence, one thread per system
+  if (threadIdx.x < 3) {
+    const int sys = threadIdx.x;
+    const int n = (sys == SYS_YZ) ? nxm : nx;
+    double *dl = B.coef + (long long)(sys * C_N + C_FACT) * nx;   // in: amkl, out: fact
+    double *du = B.coef + (long long)(sys * C_N + C_DU) * nx;
+    double *dp = B.coef + (long long)(sys * C_N + C_DP) * nx;
+    double *g = B.coef + (long long)(sys * C_N + C_G) * nx;
+    double d = 1.0;
+    dp[0] = 1.0;
+    double am_next = dl[1 < n ? 1 : 0];
+    dl[0] = 0.0;
+    double gk = 1.0;
+    g[0] = 1.0;
+    int pivot_needed = 0;
+    for (int k = 0; k < n - 1; ++k) {
+      const double am = am_next;                  // amkl(k+1), the subdiagonal of row k+1
+      if (k + 2 < n) am_next = dl[k + 2];
+      if (fabs(d) < fabs(am)) pivot_needed = 1;
+      const double fact = am / d;                 // dgttrf: FACT = DL(I)/D(I)
+      d = 1.0 - fact * du[k];                     //         D(I+1) = D(I+1) - FACT*DU(I)
+      dl[k + 1] = fact;
+      dp[k + 1] = d;
+      gk = -fact * gk;
+      g[k + 1] = gk;
+    }
+    for (int k = n; k < nx; ++k) { dl[k] = 0.0; dp[k] = 1.0; g[k] = 0.0; }
+    if (pivot_needed) atomicExch(&S->status, -2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K1: explicit terms + implicit rhs + forward elimination for all four
+// fields, one thread per (j, i) column marching k upwards.  A ring of four
+// x-planes of vx, vy, vz, temp, pr (tile + 1-cell halo) sits in shared
+// memory; plane kc+2 is fetched with cp.async while plane kc is computed.
+// Writes the RK history (rux.. = H) and the forward-sweep values y of each
+// solve; the temperature sweep starts from y(1) = 0 and the missing
+// contribution of its wall row is added by K2 (the solve is linear in y(1)).
+// ---------------------------------------------------------------------------
+constexpr int K1_TJ = 32;
+constexpr int K1_TI = 8;
+constexpr int K1_HJ = K1_TJ + 2;
+constexpr int K1_HI = K1_TI + 2;
+constexpr int K1_PL = K1_HJ * K1_HI;            // one halo plane of one field
+constexpr int K1_NSLOT = 4;
+constexpr int K1_SMEM = K1_NSLOT * F_NF * K1_PL * 8;
+
+struct RingAcc {
+  const double *ring;   // [slot][field][K1_PL]
+  int s_m, s_c, s_p;    // slots of k-1, k, k+1
+  int off;              // (ti+1)*K1_HJ + tj+1
+  __device__ __forceinline__ double operator()(int f, int dk, int dj, int di) const {
+    const int s = dk < 0 ? s_m : (dk > 0 ? s_p : s_c);
+    return ring[(s * F_NF + f) * K1_PL + off + di * K1_HJ + dj];
+  }
+};
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
+__device__ __forceinline__ void k1_load_plane(double *ring, const BoxDev &B, int p, int j0, int i0) {
+  const int slot = p & (K1_NSLOT - 1);
+  const long long poff = (long long)p * B.plane;
+  for (int idx = threadIdx.x; idx < F_NF * K1_PL; idx += blockDim.x) {
+    const int f = idx / K1_PL;
+    const int r = idx - f * K1_PL;
+    const int hi = r / K1_HJ;
+    const int hj = r - hi * K1_HJ;
+    int j = j0 + hj - 1; j = (j + B.nym) % B.nym;
+    int i = i0 + hi - 1; i = (i + B.nzm) % B.nzm;
+    const double *src = (f == F_VX ? B.vx : f == F_VY ? B.vy : f == F_VZ ? B.vz : f == F_T ? B.temp : B.pr);
+    cp_async8(ring + (slot * F_NF + f) * K1_PL + r, src + poff + (long long)i * B.nym + j);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_explicit_implicit_fwd(BatchDev bt, int ns) {
+  extern __shared__ double ring[];
+  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
+  const BoxDev &B = bt.boxes[b];
+  if (!B.active || ns >= B.nsst) return;
+  const BoxScalars *S = B.sc;
+  if (S->status != 0) return;
+  const int tile = blockIdx.x - __ldg(bt.tile_off + b);
+  const int ntj = (B.nym + K1_TJ - 1) / K1_TJ;
+  const int j0 = (tile % ntj) * K1_TJ;
+  const int i0 = (tile / ntj) * K1_TI;
+  const int tj = threadIdx.x % K1_TJ;
+  const int ti = threadIdx.x / K1_TJ;
+  const int j = j0 + tj, i = i0 + ti;
+  const bool inside = (j < B.nym) && (i < B.nzm);
+  const long long col = (long long)i * B.nym + j;
+  const int nx = B.nx, nxm = B.nxm;
+  const StencilConst c = make_sconst(B);
+  const double al = S->al, ga = S->ga, ro = S->ro, dt = S->dt;
+  const double alre = al / B.ren;
+  const double alpec = al / B.pec;
+  const double udy_al = B.dy * al;
+
+  const double *cX_sc = coefp(B, SYS_X, C_SC), *cX_f = coefp(B, SYS_X, C_FACT);
+  const double *cY_sc = coefp(B, SYS_YZ, C_SC), *cY_f = coefp(B, SYS_YZ, C_FACT);
+  const double *cT_sc = coefp(B, SYS_T, C_SC), *cT_f = coefp(B, SYS_T, C_FACT);
+
+  RingAcc acc;
+  acc.ring = ring;
+  acc.off = (ti + 1) * K1_HJ + tj + 1;
+
+  // forward-sweep carries
+  double yX = inside ? B.wall[col] : 0.0;   // rhs(1,j,i) left by the last vz solve
+  double yY = 0.0, yZ = 0.0, yT = 0.0;
+
+  k1_load_plane(ring, B, 0, j0, i0);
+  k1_load_plane(ring, B, 1, j0, i0);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+
+  for (int kc = 0; kc < nxm; ++kc) {
+    if (kc + 2 <= nx - 1) { k1_load_plane(ring, B, kc + 2, j0, i0); }
+    cp_async_commit();
+    acc.s_c = kc & 3;
+    acc.s_m = (kc + 3) & 3;   // kc-1 (unused at kc = 0 except through dkm = 0)
+    acc.s_p = (kc + 1) & 3;
+    if (inside) {
+      const long long o = (long long)kc * B.plane + col;
+      const int dkm = kc == 0 ? 0 : -1;
+      const int dkp = kc == nxm - 1 ? 0 : 1;
+      const double udx3m_k = tabk(B, T_UDX3M, kc);
+      // vy, vz: rows kc = 0..nxm-1 of the size-nxm systems
+      {
+        const double H = h_vy(acc, c, udx3m_k, dkm, dkp);
+        const double Hold = B.ruy[o];
+        const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
+        const double r = rhs_vyz(H, Hold, acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0), acc(F_VY, dkm, 0, 0),
+                                 tabk(B, T_AM3SK, kc), tabk(B, T_AC3SK, kc), tabk(B, T_AP3SK, kc),
+                                 dyp, ga, ro, alre, dt);
+        B.ruy[o] = H;
+        const double bb = r * __ldg(cY_sc + kc);
+        yY = (kc == 0) ? bb : bb - __ldg(cY_f + kc) * yY;
+        B.ybuf[1][o] = yY;
+      }
+      {
+        const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
+        const double Hold = B.ruz[o];
+        const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * B.dz * al;
+        const double r = rhs_vyz(H, Hold, acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0), acc(F_VZ, dkm, 0, 0),
+                                 tabk(B, T_AM3SK, kc), tabk(B, T_AC3SK, kc), tabk(B, T_AP3SK, kc),
+                                 dzp, ga, ro, alre, dt);
+        B.ruz[o] = H;
+        const double bb = r * __ldg(cY_sc + kc);
+        yZ = (kc == 0) ? bb : bb - __ldg(cY_f + kc) * yZ;
+        B.ybuf[2][o] = yZ;
+      }
+      if (kc >= 1) {
+        const double udx3c_k = tabk(B, T_UDX3C, kc);
+        {
+          const double H = h_vx(acc, c, udx3c_k);
+          const double Hold = B.rux[o];
+          const double r = rhs_vx(H, Hold, acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0), acc(F_VX, -1, 0, 0),
+                                  acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
+                                  tabk(B, T_AM3CK, kc), tabk(B, T_AC3CK, kc), tabk(B, T_AP3CK, kc),
+                                  al, ga, ro, alre, dt, udx3c_k);
+          B.rux[o] = H;
+          const double bb = r * __ldg(cX_sc + kc);
+          yX = bb - __ldg(cX_f + kc) * yX;
+          B.ybuf[0][o] = yX;
+        }
+        {
+          const double H = h_temp(acc, c, udx3c_k);
+          const double Hold = B.rutemp[o];
+          const double r = rhs_temp(H, Hold, acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0), acc(F_T, -1, 0, 0),
+                                    tabk(B, T_AM3CK, kc), tabk(B, T_AC3CK, kc), tabk(B, T_AP3CK, kc),
+                                    ga, ro, alpec, dt);
+          B.rutemp[o] = H;
+          const double bb = r * __ldg(cT_sc + kc);
+          yT = bb - __ldg(cT_f + kc) * yT;
+          B.ybuf[3][o] = yT;
+        }
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: backward substitution and update (SolveImpEqnUpdate_*: dgttrs back
+// sweep, q += dq), then the wall conditions of ImplicitAndUpdateVX.F90:76-77
+// and ImplicitAndUpdateTemp.F90:69-73.  One thread per column.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_implicit_bwd(BatchDev bt, int ns) {
+  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
+  const BoxDev &B = bt.boxes[b];
+  if (!B.active || ns >= B.nsst) return;
+  if (B.sc->status != 0) return;
+  const long long col = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
+  if (col >= B.plane) return;
+  const int nx = B.nx, nxm = B.nxm;
+  const long long P = B.plane;
+  const double *dX = coefp(B, SYS_X, C_DP), *uX = coefp(B, SYS_X, C_DU);
+  const double *dY = coefp(B, SYS_YZ, C_DP), *uY = coefp(B, SYS_YZ, C_DU);
+  const double *dT = coefp(B, SYS_T, C_DP), *uT = coefp(B, SYS_T, C_DU), *gT = coefp(B, SYS_T, C_G);
+  double xX = 0.0, xY = 0.0, xZ = 0.0;
+  for (int k = nxm - 1; k >= 0; --k) {
+    const long long o = (long long)k * P + col;
+    const double dy_ = __ldg(dY + k);
+    if (k == nxm - 1) {
+      xY = B.ybuf[1][o] / dy_;
+      xZ = B.ybuf[2][o] / dy_;
+    } else {
+      const double u = __ldg(uY + k);
+      xY = (B.ybuf[1][o] - u * xY) / dy_;
+      xZ = (B.ybuf[2][o] - u * xZ) / dy_;
+    }
+    B.vy[o] = B.vy[o] + xY;
+    B.vz[o] = B.vz[o] + xZ;
+    if (k >= 1) {
+      xX = (B.ybuf[0][o] - __ldg(uX + k) * xX) / __ldg(dX + k);
+      B.vx[o] = B.vx[o] + xX;
+    }
+  }
+  B.vx[col] = 0.0;
+  B.vx[(long long)(nx - 1) * P + col] = 0.0;
+  const double w = xZ;            // rhs(1,j,i) after the vz solve
+  B.wall[col] = w;
+  double xT = 0.0;
+  for (int k = nxm - 1; k >= 1; --k) {
+    const long long o = (long long)k * P + col;
+    const double y = B.ybuf[3][o] + __ldg(gT + k) * w;
+    xT = (y - __ldg(uT + k) * xT) / __ldg(dT + k);
+    B.temp[o] = B.temp[o] + xT;
+  }
+  B.temp[col] = B.tempbp;
+  B.temp[(long long)(nx - 1) * P + col] = B.temptp;
+}
+
+// ---------------------------------------------------------------------------
+// Projection: CorrectVelocity.F90:19-44 and CorrectPressure.F90:19-51 in one
+// pass over the cells k = 1..nxm.  Thread per cell.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_correct(BatchDev bt, int ns, int do_vel, int do_pr) {
+  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
+  const BoxDev &B = bt.boxes[b];
+  if (!B.active || ns >= B.nsst) return;
+  const BoxScalars *S = B.sc;
+  if (S->status != 0) return;
+  const long long cell = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
+  const long long P = B.plane;
+  if (cell >= (long long)B.nxm * P) return;
+  const int k = (int)(cell / P);
+  const long long col = cell - (long long)k * P;
+  const int i = (int)(col / B.nym);
+  const int j = (int)(col - (long long)i * B.nym);
+  const int nym = B.nym, nzm = B.nzm;
+  const int im = i == 0 ? nzm - 1 : i - 1, ip = i == nzm - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? nym - 1 : j - 1, jp = j == nym - 1 ? 0 : j + 1;
+  const int km = k == 0 ? 0 : k - 1;                 // kmv
+  const int kp = k == B.nxm - 1 ? k : k + 1;         // kpv
+  const double *phi = B.phi;
+  const double f = phi[cell];
+  const double al = S->al, dt = S->dt;
+  if (do_vel) {
+    const double udy = al * dt * B.dy;
+    const double udz = al * dt * B.dz;
+    const double usukm = al * dt * tabk(B, T_UDX3C, k);
+    if (k >= 1) B.vx[cell] = B.vx[cell] - (f - phi[(long long)km * P + col]) * usukm;
+    B.vy[cell] = B.vy[cell] - (f - phi[(long long)k * P + (long long)i * nym + jm]) * udy;
+    B.vz[cell] = B.vz[cell] - (f - phi[(long long)k * P + (long long)im * nym + j]) * udz;
+  }
+  if (do_pr) {
+    const double be = al * S->beta;
+    const double amm = tabk(B, T_AMPHK, k), acc = tabk(B, T_ACPHK, k), app = tabk(B, T_APPHK, k);
+    const long long pk = (long long)k * P;
+    const double zz = (phi[pk + (long long)ip * nym + j] - 2.0 * f + phi[pk + (long long)im * nym + j]) * B.dzq;
+    const double yy = (phi[pk + (long long)i * nym + jp] - 2.0 * f + phi[pk + (long long)i * nym + jm]) * B.dyq;
+    const double xx = phi[(long long)kp * P + col] * app + f * acc + phi[(long long)km * P + col] * amm;
+    B.pr[cell] = B.pr[cell] + f - be * (zz + yy + xx);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Divergence into the phi buffer (CalcLocalDivergence.F90:20-40); used by the
+// routine-level entry point (the fused path computes it inside the y-FFT).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double local_div(const BoxDev &B, int k, int j, int i) {
+  const long long P = B.plane;
+  const int nym = B.nym, nzm = B.nzm;
+  const int ip = i == nzm - 1 ? 0 : i + 1;
+  const int jp = j == nym - 1 ? 0 : j + 1;
+  const long long o = (long long)k * P + (long long)i * nym + j;
+  return (B.vz[(long long)k * P + (long long)ip * nym + j] - B.vz[o]) * B.dz
+       + (B.vy[(long long)k * P + (long long)i * nym + jp] - B.vy[o]) * B.dy
+       + (B.vx[o + P] - B.vx[o]) * tabk(B, T_UDX3M, k);
+}
+
+__global__ void __launch_bounds__(256) k_divergence(BatchDev bt) {
+  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
+  const BoxDev &B = bt.boxes[b];
+  if (!B.active) return;
+  const BoxScalars *S = B.sc;
+  const long long cell = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
+  const long long P = B.plane;
+  if (cell >= (long long)B.nxm * P) return;
+  const int k = (int)(cell / P);
+  const long long col = cell - (long long)k * P;
+  const int i = (int)(col / B.nym);
+  const int j = (int)(col - (long long)i * B.nym);
+  const double usdtal = 1.0 / (S->dt * S->al);
+  B.phi[cell] = local_div(B, k, j, i) * usdtal;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics over the current velocity: CFL (CalcMaxCFL.F90:29-39), max
+// |div| (CheckDivergence.F90:29-38) and vmax (GlobalQuantities.F90:44-46).
+// Block max + atomicMax on the bit pattern (values are >= 0).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void __launch_bounds__(256) k_diag(BatchDev bt) {
+  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
+  const BoxDev &B = bt.boxes[b];
+  if (!B.active) return;
+  BoxScalars *S = B.sc;
+  if (S->status != 0) return;
+  const long long P = B.plane;
+  const long long n = (long long)B.nxm * P;
+  const long long base = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x * 4;
+  double cfl = 0.0, dv = 0.0, vy = 0.0, vz = 0.0;
+  int bad = 0;
+  for (int r = 0; r < 4; ++r) {
+    const long long cell = base + r * blockDim.x + threadIdx.x;
+    if (cell >= n) break;
+    const int k = (int)(cell / P);
+    const long long col = cell - (long long)k * P;
+    const int i = (int)(col / B.nym);
+    const int j = (int)(col - (long long)i * B.nym);
+    const int ip = i == B.nzm - 1 ? 0 : i + 1;
+    const int jp = j == B.nym - 1 ? 0 : j + 1;
+    const double udx3m = tabk(B, T_UDX3M, k);
+    const double vzc = B.vz[cell], vzp = B.vz[(long long)k * P + (long long)ip * B.nym + j];
+    const double vyc = B.vy[cell], vyp = B.vy[(long long)k * P + (long long)i * B.nym + jp];
+    const double vxc = B.vx[cell], vxp = B.vx[cell + P];
+    const double q = fabs((vzc + vzp) * 0.5 * B.dz) + fabs((vyc + vyp) * 0.5 * B.dy)
+                   + fabs((vxc + vxp) * 0.5 * udx3m);
+    const double d = (vzp - vzc) * B.dz + (vyp - vyc) * B.dy + (vxp - vxc) * udx3m;
+    if (!isfinite(q) || !isfinite(d) || !isfinite(B.temp[cell])) bad = 1;
+    cfl = fmax(cfl, q);
+    dv = fmax(dv, fabs(d));
+    vy = fmax(vy, fabs(vyc));
+    vz = fmax(vz, fabs(vzc));
+  }
+  cfl = warp_max(cfl); dv = warp_max(dv); vy = warp_max(vy); vz = warp_max(vz);
+  __shared__ double sm[4][8];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sm[0][w] = cfl; sm[1][w] = dv; sm[2][w] = vy; sm[3][w] = vz; }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&S->nonfinite, 1);
+  if (threadIdx.x < 4) {
+    double m = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) m = fmax(m, sm[threadIdx.x][q]);
+    atomicMax(&S->red_u64[threadIdx.x], dbits(m));
+  }
+}
+
+// Plate Nusselt numbers (CalcPlateNu.F90:24-43): per-block partial sums, in a
+// fixed number of blocks per box so that the final sum order is fixed.
+constexpr int NU_BLOCKS = 32;
+__global__ void __launch_bounds__(256) k_plate_nu(const BoxDev *__restrict__ boxes, int nbox) {
+  const int b = blockIdx.y;
+  if (b >= nbox) return;
+  const BoxDev &B = boxes[b];
+  if (!B.active) return;
+  const long long P = B.plane;
+  const int nx = B.nx, nxm = B.nxm;
+  const double del = 1.0 / (tabk(B, T_XC, 1) - tabk(B, T_XC, 0));
+  const double deln = 1.0 / (tabk(B, T_XC, nx - 1) - tabk(B, T_XC, nxm - 1));
+  double lo = 0.0, up = 0.0;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P; c += (long long)NU_BLOCKS * blockDim.x) {
+    lo += (B.temp[c] - B.temp[P + c]) * del;
+    up += (B.temp[(long long)(nxm - 1) * P + c] - B.temp[(long long)(nx - 1) * P + c]) * deln;
+  }
+  __shared__ double s_lo[256], s_up[256];
+  s_lo[threadIdx.x] = lo; s_up[threadIdx.x] = up;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) { s_lo[threadIdx.x] += s_lo[threadIdx.x + st]; s_up[threadIdx.x] += s_up[threadIdx.x + st]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { B.nu_part[2 * blockIdx.x] = s_lo[0]; B.nu_part[2 * blockIdx.x + 1] = s_up[0]; }
+}
+
+// Finalise the reductions of one box (thread per box): diagnostics, plate Nu
+// and the reference's error codes.
+//   mode 0: step start  -> cfl/div/vmax from k_diag, then the dt rule of
+//           main.F90:171-189 (codes 165, 166)
+//   mode 1: step end    -> time += dt, ntime += 1, plate Nu, velocity limit
+//           (266, main.F90:204) and non-finite values (266)
+__global__ void k_finalize(const BoxDev *__restrict__ boxes, int nbox, int mode) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbox) return;
+  const BoxDev &B = boxes[b];
+  if (!B.active) return;
+  BoxScalars *S = B.sc;
+  if (mode == 0) {
+    if (S->status != 0) return;
+    double cfl = __longlong_as_double((long long)S->red_u64[0]);
+    S->divmax = __longlong_as_double((long long)S->red_u64[1]);
+    S->vmax[1] = __longlong_as_double((long long)S->red_u64[2]);
+    S->vmax[0] = __longlong_as_double((long long)S->red_u64[3]);
+    for (int q = 0; q < 4; ++q) S->red_u64[q] = 0ull;
+    cfl = fmax(cfl, 0.00000001);             // CalcMaxCFL.F90:21
+    S->cfl = cfl;
+    if (S->nonfinite) { S->status = 266; return; }
+    // velocity limit (main.F90:204) and mass conservation (main.F90:220)
+    if (S->vmax[0] > S->limitvel && S->vmax[1] > S->limitvel) { S->status = 266; return; }
+    if (S->ntime >= 1 && S->resid > 0.0 && S->divmax > S->resid) { S->status = 169; return; }
+    double dt = S->dt;
+    if (S->idtv) {
+      if (S->ntime > 1) {
+        dt = (cfl < 1.0e-8) ? S->dtmax : S->cflmax / cfl;
+        if (dt > S->dtmax) dt = S->dtmax;
+      } else {
+        dt = S->dtmin;
+      }
+      S->dt = dt;
+      S->cfl_used = cfl;
+      if (dt < S->dtmin) S->status = 166;
+    } else {
+      S->cfl_used = cfl * dt;
+      if (S->cfl_used > S->cflmax) S->status = 165;
+    }
+  } else {
+    if (S->status != 0) return;
+    S->time += S->dt;
+    S->ntime += 1;
+    double lo = 0.0, up = 0.0;
+    for (int q = 0; q < NU_BLOCKS; ++q) { lo += B.nu_part[2 * q]; up += B.nu_part[2 * q + 1]; }
+    S->nu_bot = lo / (double)(B.nzm * B.nym);
+    S->nu_top = up / (double)(B.nzm * B.nym);
+    if (!isfinite(S->nu_bot) || !isfinite(S->nu_top)) S->status = 266;
+    if (B.hist_cap > 0) {
+      double *h = B.hist + (long long)((S->ntime - 1) % B.hist_cap) * HIST_FIELDS;
+      h[0] = S->time; h[1] = S->dt; h[2] = S->cfl_used; h[3] = S->divmax;
+      h[4] = S->nu_bot; h[5] = S->nu_top; h[6] = S->vmax[1]; h[7] = S->vmax[0];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the reference's Fortran order q(k, j, i) (k
+// fastest, nk rows) and the device order q[k][i][j].  32x32 smem tiles over
+// (k, j) for each i.
+// ---------------------------------------------------------------------------
+__global__ void k_fortran_to_dev(const double *__restrict__ src, double *__restrict__ dst,
+                                 int nk, int nym, int nzm, int ld_k) {
+  __shared__ double t[32][33];
+  const int i = blockIdx.z;
+  const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, k = k0 + threadIdx.x;
+    if (j < nym && k < nk) t[r][threadIdx.x] = src[(long long)i * nym * ld_k + (long long)j * ld_k + k];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int k = k0 + r, j = j0 + threadIdx.x;
+    if (j < nym && k < nk) dst[(long long)k * nym * nzm + (long long)i * nym + j] = t[threadIdx.x][r];
+  }
+}
+
+__global__ void k_dev_to_fortran(const double *__restrict__ src, double *__restrict__ dst,
+                                 int nk, int nym, int nzm, int ld_k) {
+  __shared__ double t[32][33];
+  const int i = blockIdx.z;
+  const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int k = k0 + r, j = j0 + threadIdx.x;
+    if (j < nym && k < nk) t[r][threadIdx.x] = src[(long long)k * nym * nzm + (long long)i * nym + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, k = k0 + threadIdx.x;
+    if (j < nym && k < nk) dst[(long long)i * nym * ld_k + (long long)j * ld_k + k] = t[threadIdx.x][r];
+  }
+}
+
+}  // namespace afid

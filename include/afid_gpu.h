@@ -1,0 +1,162 @@
+/*
+ * afid_gpu.h -- C-ABI of the B200 implementation of AFiD's RK3 time-step
+ * hot path (FP64).
+ *
+ * The reference (PhysicsofFluids/AFiD, Fortran 90) calls its hot path as
+ * argument-less subroutines that share state through the modules `param`,
+ * `local_arrays` and `fftw_params` (param.F90:4-177), in the order of
+ * TimeMarcher.F90:32-72 and main.F90:167-221.  This library keeps those
+ * subroutine boundaries: a *box* holds the state that those modules hold for
+ * one simulation (fields, RK history, the shared rhs array's wall row, grid
+ * metrics), resident in HBM, and each routine of the reference has an entry
+ * point of the same name acting on one box.  Fused entry points advance many
+ * boxes at once.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative AFID_E* code; the
+ *     text of the last error is returned by afid_last_error().
+ *   - Host arrays are FP64 in the reference's Fortran order q(k, j, i), k
+ *     (wall-normal x) fastest: nx*nym*nzm values for vx, vy, vz, temp, pr and
+ *     the RK history, nxm*nym*nzm for dph.  No halo cells.
+ *   - Physics failures do not abort: a box whose step fails carries the
+ *     reference's error code in afid_box_scalars.status (165 CFL too large,
+ *     166 dt < dtmin, 169 divergence > resid, 266 velocity limit or a
+ *     non-finite value; main.F90:184-220) and is skipped by later launches.
+ *   - One host thread per context; calls on a context are not re-entrant.
+ *   - All work is queued on the context's stream; functions that return
+ *     host data synchronise that stream.
+ */
+#ifndef AFID_GPU_H
+#define AFID_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AFID_OK 0
+#define AFID_EINVAL (-1)    /* bad argument */
+#define AFID_ENOMEM (-2)    /* device allocation failed */
+#define AFID_ECUDA (-3)     /* CUDA runtime error */
+#define AFID_ENOBOX (-4)    /* unknown box id */
+#define AFID_EFFT (-5)      /* nym or nzm has a prime factor > 7 (main.F90:156-165, code 444) */
+#define AFID_ESIZE (-6)     /* size beyond a fixed limit of the entry point */
+
+typedef struct afid_ctx afid_ctx;
+
+/* Fields a box holds (the arrays of module local_arrays, param.F90:80-87). */
+enum afid_field {
+  AFID_VX = 0, AFID_VY = 1, AFID_VZ = 2, AFID_TEMP = 3, AFID_PR = 4,
+  AFID_RUX = 5, AFID_RUY = 6, AFID_RUZ = 7, AFID_RUTEMP = 8,
+  AFID_DPH = 9,            /* nxm rows */
+  AFID_QCAP = 10, AFID_DQ = 11, AFID_HRO = 12, AFID_RHS = 13,
+  AFID_WALL = 14           /* rhs(1, :, :): nym*nzm values, (j, i) order */
+};
+
+/* The bou.in values of one simulation (ReadInputFile.F90:16-56,
+ * MANUAL.md).  xc (nx node positions) is passed separately to
+ * afid_box_add; afid_make_grid builds it from istr3/str3. */
+typedef struct afid_box_params {
+  int nxm, nym, nzm;     /* NXM NYM NZM */
+  int nsst;              /* 3: RK3, 1: Adams-Bashforth (NSST) */
+  double alx3;           /* ALX3D */
+  double ylen, zlen;     /* YLEN ZLEN */
+  double ray, pra;       /* RA PRA */
+  int inslws, inslwn;    /* 1: no-slip, 0: stress-free lower/upper wall */
+  double tempbp, temptp; /* plate temperatures (SetTempBCs.F90: 1, 0) */
+  double dt;             /* DT: fixed dt, or the first dt when idtv = 1 */
+  int idtv;              /* IDTV: 0 fixed dt, 1 CFL-adaptive */
+  double cflmax;         /* CFLMAX */
+  double dtmin, dtmax;   /* DTMIN DTMAX */
+  double vlim;           /* VLIM */
+  double resid;          /* RESID (<= 0 disables code 169) */
+} afid_box_params;
+
+/* Per-box scalars kept on the device and updated every step. */
+typedef struct afid_box_scalars {
+  double dt;          /* time step of the last step */
+  double time;        /* simulation time */
+  double cfl;         /* CalcMaxCFL of the velocity at the start of the last step */
+  double cfl_used;    /* cfl*dt (fixed dt) or cfl (variable dt) */
+  double divmax;      /* CheckDivergence of the velocity at the start of the last step */
+  double vmax[3];     /* max |vz|, |vy|, |vx| (GlobalQuantities.F90:44-46) */
+  double nu_bot;      /* CalcPlateNu lower plate, after the last step */
+  double nu_top;      /* CalcPlateNu upper plate */
+  int ntime;          /* completed steps */
+  int status;         /* 0, or the reference error code that stopped this box */
+} afid_box_scalars;
+
+/* One per-step record of the device-side history ring (afid_box_history). */
+typedef struct afid_step_record {
+  double time, dt, cfl_used, divmax, nu_bot, nu_top, vmax_y, vmax_z;
+} afid_step_record;
+
+/* ---- library / context ------------------------------------------------ */
+int afid_version(void);
+const char *afid_last_error(void);
+int afid_ctx_create(afid_ctx **ctx, int device);
+int afid_ctx_destroy(afid_ctx *ctx);
+/* Use an external cudaStream_t (0 reverts to the context's own stream). */
+int afid_ctx_set_stream(afid_ctx *ctx, void *stream);
+void *afid_ctx_stream(afid_ctx *ctx);
+int afid_ctx_synchronize(afid_ctx *ctx);
+
+/* ---- grid and boxes ------------------------------------------------------
+ * afid_make_grid: node positions xc(1..nx) of CreateGrid.F90:66-119 for
+ * istr3 = 0 (uniform), 4 (tanh), 6 (clipped Chebyshev), plus 7 (pure
+ * Chebyshev-Gauss-Lobatto, x_k = alx3 (1 - cos(pi (k-1)/nxm)) / 2). */
+int afid_make_grid(int nxm, int istr3, double str3, double alx3, double *xc);
+/* Bytes of HBM a box of these parameters holds (for admission control). */
+size_t afid_box_device_bytes(const afid_box_params *p);
+/* Create a box: allocates its fields (zeroed, as AllocateReal3DArray does,
+ * AuxiliaryRoutines.F90:79-97) and computes its metrics (CreateGrid.F90,
+ * InitPressureSolver.F90) and time-scheme constants
+ * (InitTimeMarchScheme.F90). */
+int afid_box_add(afid_ctx *ctx, const afid_box_params *p, const double *xc, int *box_id);
+int afid_box_remove(afid_ctx *ctx, int box_id);
+int afid_box_upload(afid_ctx *ctx, int box_id, int field, const double *host);
+int afid_box_download(afid_ctx *ctx, int box_id, int field, double *host);
+/* Zero the RK history, the carried rhs wall row, time, step count and
+ * status; set dt (values <= 0 keep the current dt). */
+int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
+int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
+/* Copies up to max_records of the most recent per-step records, oldest
+ * first; returns the number copied (>= 0) or an error code. */
+int afid_box_history(afid_ctx *ctx, int box_id, afid_step_record *out, int max_records);
+
+/* ---- routine-level entry points (one box) --------------------------------
+ * Each replaces the reference subroutine of the same name.  The substep
+ * coefficients al, ga, ro, beta (TimeMarcher.F90:22-30) are set by
+ * afid_time_marcher_begin_substep from the box's dt. */
+int afid_time_marcher_begin_substep(afid_ctx *ctx, int box_id, int ns);  /* TimeMarcher.F90:22-30 */
+int afid_explicit_terms_vx(afid_ctx *ctx, int box_id);       /* ExplicitTermsVX.F90:11 */
+int afid_explicit_terms_vy(afid_ctx *ctx, int box_id);       /* ExplicitTermsVY.F90:11 */
+int afid_explicit_terms_vz(afid_ctx *ctx, int box_id);       /* ExplicitTermsVZ.F90:11 */
+int afid_explicit_terms_temp(afid_ctx *ctx, int box_id);     /* ExplicitTermsTemp.F90:11 */
+int afid_implicit_and_update_vx(afid_ctx *ctx, int box_id);  /* ImplicitAndUpdateVX.F90:14 + SolveImpEqnUpdate_X.F90:12 */
+int afid_implicit_and_update_vy(afid_ctx *ctx, int box_id);  /* ImplicitAndUpdateVY.F90:14 + SolveImpEqnUpdate_YZ.F90:12 */
+int afid_implicit_and_update_vz(afid_ctx *ctx, int box_id);  /* ImplicitAndUpdateVZ.F90:14 + SolveImpEqnUpdate_YZ.F90:12 */
+int afid_implicit_and_update_temp(afid_ctx *ctx, int box_id);/* ImplicitAndUpdateTemp.F90:13 + SolveImpEqnUpdate_Temp.F90:11 */
+int afid_calc_local_divergence(afid_ctx *ctx, int box_id);   /* CalcLocalDivergence.F90:12 */
+int afid_solve_pressure_correction(afid_ctx *ctx, int box_id); /* SolvePressureCorrection.F90:12 */
+int afid_correct_velocity(afid_ctx *ctx, int box_id);        /* CorrectVelocity.F90:11 */
+int afid_correct_pressure(afid_ctx *ctx, int box_id);        /* CorrectPressure.F90:11 */
+int afid_calc_max_cfl(afid_ctx *ctx, int box_id, double *cflm);      /* CalcMaxCFL.F90:11 */
+int afid_check_divergence(afid_ctx *ctx, int box_id, double *qmax);  /* CheckDivergence.F90:11 */
+int afid_calc_plate_nu(afid_ctx *ctx, int box_id, double *nuslow, double *nusupp); /* CalcPlateNu.F90:11 */
+
+/* ---- fused fast path over a set of boxes ---------------------------------
+ * afid_step: nsteps passes of main.F90:171-200 (CalcMaxCFL, dt rule,
+ * TimeMarcher, time += dt, CalcPlateNu) for every listed box, each kernel
+ * launched once for all boxes.  afid_step_graph does the same through a
+ * CUDA graph of one step, captured on first use per box set. */
+int afid_step(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
+int afid_step_graph(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
+/* One substep ns of TimeMarcher.F90:28-72 with the current dt (no CFL). */
+int afid_substep(afid_ctx *ctx, const int *box_ids, int nbox, int ns);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFID_GPU_H */
