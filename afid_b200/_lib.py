@@ -32,8 +32,11 @@ EXPORTS = [
     "afid_implicit_and_update_temp", "afid_calc_local_divergence",
     "afid_solve_pressure_correction", "afid_correct_velocity", "afid_correct_pressure",
     "afid_calc_max_cfl", "afid_check_divergence", "afid_calc_plate_nu", "afid_step",
-    "afid_step_graph", "afid_substep",
+    "afid_step_graph", "afid_substep", "afid_step_profiled",
 ]
+
+KERNELS = ["diag", "finalize", "prep", "explicit_fwd", "implicit_bwd", "fft_y_fwd", "fft_z_fwd",
+           "poisson_x", "fft_z_inv", "fft_y_inv", "correct", "plate_nu"]
 
 
 class BoxParams(C.Structure):
@@ -101,6 +104,7 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_calc_plate_nu": ([vp, i, dp, dp], i),
         "afid_step": ([vp, ip, i, i], i), "afid_step_graph": ([vp, ip, i, i], i),
         "afid_substep": ([vp, ip, i, i], i),
+        "afid_step_profiled": ([vp, ip, i, i, dp, ip, i], i),
     }
     for name in ("explicit_terms_vx", "explicit_terms_vy", "explicit_terms_vz",
                  "explicit_terms_temp", "implicit_and_update_vx", "implicit_and_update_vy",

@@ -267,8 +267,8 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     BoxDev d = hb->dev;
     d.active = 1;
     devs.push_back(d);
-    const size_t sy = (size_t)2 * fft_y_pairs(d.nym) * d.nym * sizeof(double2);
-    const size_t sz = (size_t)2 * fft_z_lines(d.nzm) * d.nzm * sizeof(double2);
+    const size_t sy = (size_t)fft_smem_bytes(d.nym, fft_y_pairs(d.nym));
+    const size_t sz = (size_t)fft_smem_bytes(d.nzm, fft_z_lines(d.nzm));
     if (sy > bt->smem_y) bt->smem_y = sy;
     if (sz > bt->smem_z) bt->smem_z = sz;
   }
@@ -306,61 +306,99 @@ int init_kernel_attrs() {
   static bool done = false;
   if (done) return 0;
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
-  CK(cudaFuncSetAttribute(k_fft_y_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
-  CK(cudaFuncSetAttribute(k_fft_y_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
-  CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
-  CK(cudaFuncSetAttribute(k_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, FFT_SMEM_BUDGET));
+  const int fsm = 200 * 1024;   // lines x N plus twiddles, bounded by the nym, nzm <= 8192 limit
+  CK(cudaFuncSetAttribute(k_fft_y_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fft_y_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   done = true;
   return 0;
 }
 
 // ---- launch sequences ------------------------------------------------------
-int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel) {
+// Optional per-kernel timing: when ``prof`` is set, an event is recorded
+// after every launch and the elapsed times are accumulated per kernel slot.
+struct Prof {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> slot;
+  cudaStream_t s = nullptr;
+  int mark(int k) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, s));
+    ev.push_back(e);
+    slot.push_back(k);
+    return 0;
+  }
+};
+
+#define PMARK(p, k)                 \
+  do {                              \
+    if (p) {                        \
+      int r_ = (p)->mark(k);        \
+      if (r_) return r_;            \
+    }                               \
+  } while (0)
+
+int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof *pf = nullptr) {
   if (from_vel)
     k_fft_y_fwd<true><<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
   else
     k_fft_y_fwd<false><<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
   CKL();
+  PMARK(pf, AFID_K_FFT_Y_FWD);
   k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, -1);
   CKL();
+  PMARK(pf, AFID_K_FFT_Z_FWD);
   k_poisson_x<<<bt->total[FAM_PX], 256, 0, s>>>(bdev(bt, FAM_PX), ns);
   CKL();
+  PMARK(pf, AFID_K_POISSON_X);
   k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, +1);
   CKL();
+  PMARK(pf, AFID_K_FFT_Z_INV);
   k_fft_y_inv<<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
   CKL();
+  PMARK(pf, AFID_K_FFT_Y_INV);
   return 0;
 }
 
-int launch_substep(const Batch *bt, cudaStream_t s, int ns) {
+int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) {
   const int nb = (int)bt->ids.size();
   k_substep_prep<<<nb, 256, 0, s>>>(bt->d_boxes, nb, ns);
   CKL();
+  PMARK(pf, AFID_K_PREP);
   k_explicit_implicit_fwd<<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
   CKL();
+  PMARK(pf, AFID_K_EXPLICIT_FWD);
   k_implicit_bwd<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
   CKL();
-  int rc = launch_poisson(bt, s, ns, true);
+  PMARK(pf, AFID_K_IMPLICIT_BWD);
+  int rc = launch_poisson(bt, s, ns, true, pf);
   if (rc) return rc;
-  k_correct<<<bt->total[FAM_CELL], 256, 0, s>>>(bdev(bt, FAM_CELL), ns, 1, 1);
+  k_correct<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns, 1, 1);
   CKL();
+  PMARK(pf, AFID_K_CORRECT);
   return 0;
 }
 
-int launch_step(const Batch *bt, cudaStream_t s) {
+int launch_step(const Batch *bt, cudaStream_t s, Prof *pf = nullptr) {
   const int nb = (int)bt->ids.size();
   k_diag<<<bt->total[FAM_DIAG], 256, 0, s>>>(bdev(bt, FAM_DIAG));
   CKL();
+  PMARK(pf, AFID_K_DIAG);
   k_finalize<<<cdiv(nb, 128), 128, 0, s>>>(bt->d_boxes, nb, 0);
   CKL();
+  PMARK(pf, AFID_K_FINALIZE);
   for (int ns = 0; ns < 3; ++ns) {
-    int rc = launch_substep(bt, s, ns);
+    int rc = launch_substep(bt, s, ns, pf);
     if (rc) return rc;
   }
   k_plate_nu<<<dim3(NU_BLOCKS, nb), 256, 0, s>>>(bt->d_boxes, nb);
   CKL();
+  PMARK(pf, AFID_K_PLATE_NU);
   k_finalize<<<cdiv(nb, 128), 128, 0, s>>>(bt->d_boxes, nb, 1);
   CKL();
+  PMARK(pf, AFID_K_FINALIZE);
   return 0;
 }
 
@@ -827,7 +865,7 @@ static int correct(afid_ctx *c, int id, int vel, int pr) {
   Batch *bt;
   rc = single_batch(c, id, &bt);
   if (rc) return rc;
-  k_correct<<<bt->total[FAM_CELL], 256, 0, c->stream>>>(bdev(bt, FAM_CELL), 0, vel, pr);
+  k_correct<<<bt->total[FAM_COL], 256, 0, c->stream>>>(bdev(bt, FAM_COL), 0, vel, pr);
   CKL();
   return 0;
 }
@@ -918,6 +956,34 @@ int afid_step(afid_ctx *c, const int *ids, int n, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     rc = launch_step(bt, c->stream);
     if (rc) return rc;
+  }
+  return 0;
+}
+
+int afid_step_profiled(afid_ctx *c, const int *ids, int n, int nsteps, double *kernel_ms,
+                       int *kernel_launches, int nkernel) {
+  if (!c || !kernel_ms || nkernel < AFID_K_COUNT) return fail(AFID_EINVAL, "bad argument");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  for (int k = 0; k < nkernel; ++k) { kernel_ms[k] = 0.0; if (kernel_launches) kernel_launches[k] = 0; }
+  for (int st = 0; st < nsteps; ++st) {
+    Prof pf;
+    pf.s = c->stream;
+    rc = pf.mark(-1);
+    if (rc) return rc;
+    rc = launch_step(bt, c->stream, &pf);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t q = 1; q < pf.ev.size(); ++q) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, pf.ev[q - 1], pf.ev[q]));
+      kernel_ms[pf.slot[q]] += ms;
+      if (kernel_launches) kernel_launches[pf.slot[q]] += 1;
+    }
+    for (auto e : pf.ev) cudaEventDestroy(e);
   }
   return 0;
 }

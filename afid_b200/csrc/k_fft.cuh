@@ -7,10 +7,10 @@
 // The 2DECOMP pencil transposes of the reference disappear: each transform
 // reads its lines directly from the plane-major layout.
 //
-// The FFTs are Stockham auto-sort passes of radix 4, 2, 3, 5 (7 and any other
-// radix through the twiddle table) in shared memory, ping-ponging between two
-// buffers.  Twiddles exp(-2 pi i n / N) come from a table computed on the host
-// in extended precision.
+// The FFTs are Stockham auto-sort passes of radix 4, 2, 3, 5 and 7 in shared
+// memory, ping-ponging between two buffers.  Twiddles exp(-2 pi i n / N) come
+// from a table computed on the host in extended precision and copied to
+// shared memory by every block.
 #pragma once
 #include "afid_device.cuh"
 
@@ -18,7 +18,7 @@ namespace afid {
 
 // radix-R butterfly on v[0..R-1] (unnormalised DFT, exponent sign ``sgn``)
 template <int R>
-__device__ __forceinline__ void dft_small(double2 *v, int sgn, const double2 *__restrict__ tw, int N) {
+__device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double2 *tw, int N) {
   if (R == 2) {
     const double2 a = v[0], b = v[1];
     v[0] = cadd(a, b);
@@ -68,7 +68,7 @@ __device__ __forceinline__ void dft_small(double2 *v, int sgn, const double2 *__
       double2 acc = v[0];
 #pragma unroll
       for (int m = 1; m < R; ++m) {
-        double2 w = __ldg(&tw[((m * q) % R) * step]);
+        double2 w = tw[((m * q) % R) * step];
         if (sgn > 0) w.y = -w.y;
         acc = cadd(acc, cmul(v[m], w));
       }
@@ -79,16 +79,19 @@ __device__ __forceinline__ void dft_small(double2 *v, int sgn, const double2 *__
   }
 }
 
-// One Stockham pass of radix R over L lines of length N.
-// LINE_MAJOR: element (l, n) at l*N + n, else at n*L + l.
+// One Stockham pass of radix R over L lines of length N, from buffer a into
+// buffer b (both in shared memory).  LINE_MAJOR: element (l, n) at l*N + n,
+// else at n*L + l.
+constexpr int FFT_T = 256;          // threads per FFT block
+constexpr int FFT_ELEMS = 3072;     // lines x N per block (two buffers: 96 KB)
+
 template <int R, bool LINE_MAJOR>
 __device__ __forceinline__ void stockham_pass(const double2 *__restrict__ a, double2 *__restrict__ b,
-                                              int N, int L, int Ns, int sgn,
-                                              const double2 *__restrict__ tw) {
+                                              int N, int L, int Ns, int sgn, const double2 *tw) {
   const int NR = N / R;
   const int tstr = N / (Ns * R);
   const int total = NR * L;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+  for (int t = threadIdx.x; t < total; t += FFT_T) {
     int l, j;
     if (LINE_MAJOR) { j = t % NR; l = t / NR; } else { l = t % L; j = t / L; }
     const int k = j % Ns;
@@ -101,7 +104,7 @@ __device__ __forceinline__ void stockham_pass(const double2 *__restrict__ a, dou
     if (Ns > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        double2 w = __ldg(&tw[r * k * tstr]);
+        double2 w = tw[r * k * tstr];
         if (sgn > 0) w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
@@ -119,7 +122,7 @@ __device__ __forceinline__ void stockham_pass(const double2 *__restrict__ a, dou
 // Full transform; returns the buffer holding the result.
 template <bool LINE_MAJOR>
 __device__ double2 *stockham(double2 *a, double2 *b, int N, int L, const int *rad, int np,
-                             int sgn, const double2 *__restrict__ tw) {
+                             int sgn, const double2 *tw) {
   int Ns = 1;
   for (int p = 0; p < np; ++p) {
     const int R = rad[p];
@@ -137,20 +140,23 @@ __device__ double2 *stockham(double2 *a, double2 *b, int N, int L, const int *ra
   return a;
 }
 
-// Number of row pairs per block of the y transforms and ky columns per block
-// of the z transform, chosen on the host per box (kept in sync with these
-// formulas by afid_capi.cu).
-constexpr int FFT_SMEM_BUDGET = 96 * 1024;   // bytes for the two ping-pong buffers
+// Lines per block: row pairs of the y transforms, ky columns of the z
+// transform.  Shared memory per block: two (lines x N) complex buffers plus
+// the N twiddles.
 __host__ __device__ __forceinline__ int fft_y_pairs(int nym) {
-  int p = FFT_SMEM_BUDGET / (2 * 16 * nym);
+  int p = FFT_ELEMS / nym;
   if (p > 8) p = 8;
   if (p < 1) p = 1;
   return p;
 }
 __host__ __device__ __forceinline__ int fft_z_lines(int nzm) {
-  int l = 1;
-  while (l < 16 && 2 * (2 * l) * 16 * nzm <= FFT_SMEM_BUDGET) l *= 2;
+  int l = FFT_ELEMS / nzm;
+  if (l > 16) l = 16;
+  if (l < 1) l = 1;
   return l;
+}
+__host__ __device__ __forceinline__ int fft_smem_bytes(int n, int lines) {
+  return (2 * lines + 1) * n * 16;
 }
 
 // ---------------------------------------------------------------------------
@@ -159,7 +165,7 @@ __host__ __device__ __forceinline__ int fft_z_lines(int nzm) {
 // computed on the fly; otherwise they are read from phi (the dph buffer).
 // ---------------------------------------------------------------------------
 template <bool FROM_VEL>
-__global__ void __launch_bounds__(256) k_fft_y_fwd(BatchDev bt, int ns) {
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
@@ -172,7 +178,8 @@ __global__ void __launch_bounds__(256) k_fft_y_fwd(BatchDev bt, int ns) {
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / groups;
   const int i0 = (tile - k * groups) * 2 * Pp;
-  double2 *a = fsm, *bb = fsm + Pp * N;
+  double2 *a = fsm, *bb = fsm + Pp * N, *tws = fsm + 2 * Pp * N;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = __ldg(B.twy + t);
   const long long P = B.plane;
   const double usdtal = FROM_VEL ? 1.0 / (S->dt * S->al) : 0.0;
   const double udx3m = FROM_VEL ? tabk(B, T_UDX3M, k) : 0.0;
@@ -197,7 +204,7 @@ __global__ void __launch_bounds__(256) k_fft_y_fwd(BatchDev bt, int ns) {
     if (row & 1) a[p * N + j].y = v; else a[p * N + j].x = v;
   }
   __syncthreads();
-  double2 *r = stockham<true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, B.twy);
+  const double2 *r = stockham<true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, tws);
   const int nh = B.nymh;
   for (int t = threadIdx.x; t < Pp * nh; t += blockDim.x) {
     const int p = t / nh, q = t - p * nh;
@@ -217,7 +224,7 @@ __global__ void __launch_bounds__(256) k_fft_y_fwd(BatchDev bt, int ns) {
 // z transform in place on spec[k][kz][ky] for a tile of L consecutive ky.
 // Forward transforms divide by nym*nzm (SolvePressureCorrection.F90:105).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fft_z(BatchDev bt, int ns, int sgn) {
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
@@ -229,7 +236,8 @@ __global__ void __launch_bounds__(256) k_fft_z(BatchDev bt, int ns, int sgn) {
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / ntl;
   const int ky0 = (tile - k * ntl) * L;
-  double2 *a = fsm, *bb = fsm + L * N;
+  double2 *a = fsm, *bb = fsm + L * N, *tws = fsm + 2 * L * N;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = __ldg(B.twz + t);
   double2 *spec = B.spec + (long long)k * N * nh;
   for (int t = threadIdx.x; t < L * N; t += blockDim.x) {
     const int l = t % L, n = t / L;
@@ -237,7 +245,7 @@ __global__ void __launch_bounds__(256) k_fft_z(BatchDev bt, int ns, int sgn) {
     a[n * L + l] = ky < nh ? spec[(long long)n * nh + ky] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  double2 *r = stockham<false>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, B.twz);
+  const double2 *r = stockham<false>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, tws);
   const double norm = (double)(B.nzm * B.nym);
   for (int t = threadIdx.x; t < L * N; t += blockDim.x) {
     const int l = t % L, n = t / L;
@@ -324,7 +332,7 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
 // As in a c2r transform, the imaginary parts of the ky = 0 and ky = nym/2
 // coefficients are ignored.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fft_y_inv(BatchDev bt, int ns) {
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
@@ -336,7 +344,8 @@ __global__ void __launch_bounds__(256) k_fft_y_inv(BatchDev bt, int ns) {
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / groups;
   const int i0 = (tile - k * groups) * 2 * Pp;
-  double2 *a = fsm, *bb = fsm + Pp * N;
+  double2 *a = fsm, *bb = fsm + Pp * N, *tws = fsm + 2 * Pp * N;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = __ldg(B.twy + t);
   const bool even = (N % 2) == 0;
   for (int t = threadIdx.x; t < Pp * N; t += blockDim.x) {
     const int p = t / N, n = t - p * N;
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(256) k_fft_y_inv(BatchDev bt, int ns) {
     a[p * N + n] = make_double2(A.x - Bv.y, A.y + Bv.x);
   }
   __syncthreads();
-  double2 *r = stockham<true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, +1, B.twy);
+  const double2 *r = stockham<true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, +1, tws);
   const long long P = B.plane;
   for (int t = threadIdx.x; t < 2 * Pp * N; t += blockDim.x) {
     const int row = t / N, j = t - row * N;

@@ -240,9 +240,18 @@ constexpr int K1_TJ = 32;
 constexpr int K1_TI = 8;
 constexpr int K1_HJ = K1_TJ + 2;
 constexpr int K1_HI = K1_TI + 2;
-constexpr int K1_PL = K1_HJ * K1_HI;            // one halo plane of one field
+constexpr int K1_PL = K1_HJ * K1_HI;            // one halo plane of one field (340)
+constexpr int K1_NT = K1_TJ * K1_TI;            // threads per block (256)
 constexpr int K1_NSLOT = 4;
-constexpr int K1_SMEM = K1_NSLOT * F_NF * K1_PL * 8;
+constexpr int K1_NTAB = 14;                     // per-k scalars staged per plane
+constexpr int K1_RING = K1_NSLOT * F_NF * K1_PL;        // doubles
+constexpr int K1_HIST = 2 * 4 * K1_NT;                  // doubles
+constexpr int K1_TABR = 2 * 16;                         // doubles
+constexpr int K1_SMEM = (K1_RING + K1_HIST + K1_TABR) * 8;
+
+// per-k scalar slots staged in shared memory
+enum K1Tab { KT_UDX3M = 0, KT_UDX3C, KT_AM3SK, KT_AC3SK, KT_AP3SK, KT_AM3CK, KT_AC3CK, KT_AP3CK,
+             KT_XSC, KT_XF, KT_YSC, KT_YF, KT_TSC, KT_TF };
 
 struct RingAcc {
   const double *ring;   // [slot][field][K1_PL]
@@ -261,47 +270,102 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
-__device__ __forceinline__ void k1_load_plane(double *ring, const BoxDev &B, int p, int j0, int i0) {
-  const int slot = p & (K1_NSLOT - 1);
-  const long long poff = (long long)p * B.plane;
-  for (int idx = threadIdx.x; idx < F_NF * K1_PL; idx += blockDim.x) {
-    const int f = idx / K1_PL;
-    const int r = idx - f * K1_PL;
-    const int hi = r / K1_HJ;
-    const int hj = r - hi * K1_HJ;
-    int j = j0 + hj - 1; j = (j + B.nym) % B.nym;
-    int i = i0 + hi - 1; i = (i + B.nzm) % B.nzm;
-    const double *src = (f == F_VX ? B.vx : f == F_VY ? B.vy : f == F_VZ ? B.vz : f == F_T ? B.temp : B.pr);
-    cp_async8(ring + (slot * F_NF + f) * K1_PL + r, src + poff + (long long)i * B.nym + j);
+__device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int k) {
+  switch (t) {
+    case KT_UDX3M: return B.tab + (long long)T_UDX3M * B.nx + k;
+    case KT_UDX3C: return B.tab + (long long)T_UDX3C * B.nx + k;
+    case KT_AM3SK: return B.tab + (long long)T_AM3SK * B.nx + k;
+    case KT_AC3SK: return B.tab + (long long)T_AC3SK * B.nx + k;
+    case KT_AP3SK: return B.tab + (long long)T_AP3SK * B.nx + k;
+    case KT_AM3CK: return B.tab + (long long)T_AM3CK * B.nx + k;
+    case KT_AC3CK: return B.tab + (long long)T_AC3CK * B.nx + k;
+    case KT_AP3CK: return B.tab + (long long)T_AP3CK * B.nx + k;
+    case KT_XSC: return B.coef + (long long)(SYS_X * C_N + C_SC) * B.nx + k;
+    case KT_XF: return B.coef + (long long)(SYS_X * C_N + C_FACT) * B.nx + k;
+    case KT_YSC: return B.coef + (long long)(SYS_YZ * C_N + C_SC) * B.nx + k;
+    case KT_YF: return B.coef + (long long)(SYS_YZ * C_N + C_FACT) * B.nx + k;
+    case KT_TSC: return B.coef + (long long)(SYS_T * C_N + C_SC) * B.nx + k;
+    default: return B.coef + (long long)(SYS_T * C_N + C_FACT) * B.nx + k;
   }
 }
 
-__global__ void __launch_bounds__(256) k_explicit_implicit_fwd(BatchDev bt, int ns) {
-  extern __shared__ double ring[];
+// ---------------------------------------------------------------------------
+// K1: explicit terms + implicit rhs + forward elimination for all four
+// fields, one thread per (j, i) column marching k upwards.  Shared memory
+// holds (a) a ring of four x-planes of vx, vy, vz, temp, pr (tile plus a
+// 1-cell halo), fetched two planes ahead, (b) the RK history of the next
+// plane and (c) the per-k metric and LU scalars of the next plane; all three
+// arrive through cp.async while the current plane is computed, so a plane
+// costs one barrier and no exposed load latency.  Writes the RK history
+// (rux.. = H) and the forward-sweep values y of each solve; the temperature
+// sweep starts from y(1) = 0 and the missing contribution of its wall row is
+// added by K2 (the solve is linear in y(1)).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt, int ns) {
+  extern __shared__ double k1sm[];
+  double *ring = k1sm;
+  double *hring = k1sm + K1_RING;            // [2][4][K1_NT]
+  double *tring = hring + K1_HIST;           // [2][16]
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
   const BoxScalars *S = B.sc;
   if (S->status != 0) return;
+  const int tid = threadIdx.x;
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
-  const int ntj = (B.nym + K1_TJ - 1) / K1_TJ;
+  const int nym = B.nym, nzm = B.nzm;
+  const int ntj = (nym + K1_TJ - 1) / K1_TJ;
   const int j0 = (tile % ntj) * K1_TJ;
   const int i0 = (tile / ntj) * K1_TI;
-  const int tj = threadIdx.x % K1_TJ;
-  const int ti = threadIdx.x / K1_TJ;
+  const int tj = tid % K1_TJ;
+  const int ti = tid / K1_TJ;
   const int j = j0 + tj, i = i0 + ti;
-  const bool inside = (j < B.nym) && (i < B.nzm);
-  const long long col = (long long)i * B.nym + j;
+  const bool inside = (j < nym) && (i < nzm);
+  const long long P = B.plane;
+  const long long col = (long long)i * nym + j;
   const int nx = B.nx, nxm = B.nxm;
   const StencilConst c = make_sconst(B);
   const double al = S->al, ga = S->ga, ro = S->ro, dt = S->dt;
   const double alre = al / B.ren;
   const double alpec = al / B.pec;
   const double udy_al = B.dy * al;
+  const double dz_ = B.dz;
 
-  const double *cX_sc = coefp(B, SYS_X, C_SC), *cX_f = coefp(B, SYS_X, C_FACT);
-  const double *cY_sc = coefp(B, SYS_YZ, C_SC), *cY_f = coefp(B, SYS_YZ, C_FACT);
-  const double *cT_sc = coefp(B, SYS_T, C_SC), *cT_f = coefp(B, SYS_T, C_FACT);
+  const double *fld[F_NF] = {B.vx, B.vy, B.vz, B.temp, B.pr};
+  double *hist[4] = {B.rux, B.ruy, B.ruz, B.rutemp};
+
+  // this thread's halo elements (r0 = tid always < K1_PL; r1 = tid + K1_NT if < K1_PL)
+  const int r1 = tid + K1_NT;
+  const bool has1 = r1 < K1_PL;
+  long long g0, g1 = 0;
+  {
+    int hi = tid / K1_HJ, hj = tid - hi * K1_HJ;
+    int jj = (j0 + hj - 1 + nym) % nym, ii = (i0 + hi - 1 + nzm) % nzm;
+    g0 = (long long)ii * nym + jj;
+    if (has1) {
+      hi = r1 / K1_HJ; hj = r1 - hi * K1_HJ;
+      jj = (j0 + hj - 1 + nym) % nym; ii = (i0 + hi - 1 + nzm) % nzm;
+      g1 = (long long)ii * nym + jj;
+    }
+  }
+  auto load_plane = [&](int p) {
+    double *dst = ring + (p & (K1_NSLOT - 1)) * F_NF * K1_PL;
+    const long long po = (long long)p * P;
+#pragma unroll
+    for (int f = 0; f < F_NF; ++f) {
+      cp_async8(dst + f * K1_PL + tid, fld[f] + po + g0);
+      if (has1) cp_async8(dst + f * K1_PL + r1, fld[f] + po + g1);
+    }
+  };
+  auto load_next = [&](int k) {          // history and scalars of plane k
+    double *hd = hring + (k & 1) * 4 * K1_NT;
+    if (inside) {
+      const long long o = (long long)k * P + col;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) cp_async8(hd + q * K1_NT + tid, hist[q] + o);
+    }
+    if (tid < K1_NTAB) cp_async8(tring + (k & 1) * 16 + tid, k1_tab_src(B, tid, k));
+  };
 
   RingAcc acc;
   acc.ring = ring;
@@ -311,71 +375,69 @@ __global__ void __launch_bounds__(256) k_explicit_implicit_fwd(BatchDev bt, int 
   double yX = inside ? B.wall[col] : 0.0;   // rhs(1,j,i) left by the last vz solve
   double yY = 0.0, yZ = 0.0, yT = 0.0;
 
-  k1_load_plane(ring, B, 0, j0, i0);
-  k1_load_plane(ring, B, 1, j0, i0);
+  load_plane(0);
+  load_plane(1);
+  load_next(0);
   cp_async_commit();
   cp_async_wait_all();
   __syncthreads();
 
   for (int kc = 0; kc < nxm; ++kc) {
-    if (kc + 2 <= nx - 1) { k1_load_plane(ring, B, kc + 2, j0, i0); }
+    if (kc + 2 <= nx - 1) load_plane(kc + 2);
+    if (kc + 1 <= nxm - 1) load_next(kc + 1);
     cp_async_commit();
     acc.s_c = kc & 3;
     acc.s_m = (kc + 3) & 3;   // kc-1 (unused at kc = 0 except through dkm = 0)
     acc.s_p = (kc + 1) & 3;
+    const double *tk = tring + (kc & 1) * 16;
+    const double *hk = hring + (kc & 1) * 4 * K1_NT;
     if (inside) {
-      const long long o = (long long)kc * B.plane + col;
+      const long long o = (long long)kc * P + col;
       const int dkm = kc == 0 ? 0 : -1;
       const int dkp = kc == nxm - 1 ? 0 : 1;
-      const double udx3m_k = tabk(B, T_UDX3M, kc);
+      const double udx3m_k = tk[KT_UDX3M];
+      const double am_s = tk[KT_AM3SK], ac_s = tk[KT_AC3SK], ap_s = tk[KT_AP3SK];
       // vy, vz: rows kc = 0..nxm-1 of the size-nxm systems
       {
         const double H = h_vy(acc, c, udx3m_k, dkm, dkp);
-        const double Hold = B.ruy[o];
         const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
-        const double r = rhs_vyz(H, Hold, acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0), acc(F_VY, dkm, 0, 0),
-                                 tabk(B, T_AM3SK, kc), tabk(B, T_AC3SK, kc), tabk(B, T_AP3SK, kc),
-                                 dyp, ga, ro, alre, dt);
+        const double r = rhs_vyz(H, hk[1 * K1_NT + tid], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
+                                 acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
         B.ruy[o] = H;
-        const double bb = r * __ldg(cY_sc + kc);
-        yY = (kc == 0) ? bb : bb - __ldg(cY_f + kc) * yY;
+        const double bb = r * tk[KT_YSC];
+        yY = (kc == 0) ? bb : bb - tk[KT_YF] * yY;
         B.ybuf[1][o] = yY;
       }
       {
         const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
-        const double Hold = B.ruz[o];
-        const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * B.dz * al;
-        const double r = rhs_vyz(H, Hold, acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0), acc(F_VZ, dkm, 0, 0),
-                                 tabk(B, T_AM3SK, kc), tabk(B, T_AC3SK, kc), tabk(B, T_AP3SK, kc),
-                                 dzp, ga, ro, alre, dt);
+        const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
+        const double r = rhs_vyz(H, hk[2 * K1_NT + tid], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
+                                 acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
         B.ruz[o] = H;
-        const double bb = r * __ldg(cY_sc + kc);
-        yZ = (kc == 0) ? bb : bb - __ldg(cY_f + kc) * yZ;
+        const double bb = r * tk[KT_YSC];
+        yZ = (kc == 0) ? bb : bb - tk[KT_YF] * yZ;
         B.ybuf[2][o] = yZ;
       }
       if (kc >= 1) {
-        const double udx3c_k = tabk(B, T_UDX3C, kc);
+        const double udx3c_k = tk[KT_UDX3C];
+        const double am_c = tk[KT_AM3CK], ac_c = tk[KT_AC3CK], ap_c = tk[KT_AP3CK];
         {
           const double H = h_vx(acc, c, udx3c_k);
-          const double Hold = B.rux[o];
-          const double r = rhs_vx(H, Hold, acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0), acc(F_VX, -1, 0, 0),
-                                  acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
-                                  tabk(B, T_AM3CK, kc), tabk(B, T_AC3CK, kc), tabk(B, T_AP3CK, kc),
-                                  al, ga, ro, alre, dt, udx3c_k);
+          const double r = rhs_vx(H, hk[0 * K1_NT + tid], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
+                                  acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
+                                  am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
           B.rux[o] = H;
-          const double bb = r * __ldg(cX_sc + kc);
-          yX = bb - __ldg(cX_f + kc) * yX;
+          const double bb = r * tk[KT_XSC];
+          yX = bb - tk[KT_XF] * yX;
           B.ybuf[0][o] = yX;
         }
         {
           const double H = h_temp(acc, c, udx3c_k);
-          const double Hold = B.rutemp[o];
-          const double r = rhs_temp(H, Hold, acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0), acc(F_T, -1, 0, 0),
-                                    tabk(B, T_AM3CK, kc), tabk(B, T_AC3CK, kc), tabk(B, T_AP3CK, kc),
-                                    ga, ro, alpec, dt);
+          const double r = rhs_temp(H, hk[3 * K1_NT + tid], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
+                                    acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
           B.rutemp[o] = H;
-          const double bb = r * __ldg(cT_sc + kc);
-          yT = bb - __ldg(cT_f + kc) * yT;
+          const double bb = r * tk[KT_TSC];
+          yT = bb - tk[KT_TF] * yT;
           B.ybuf[3][o] = yT;
         }
       }
@@ -390,6 +452,8 @@ __global__ void __launch_bounds__(256) k_explicit_implicit_fwd(BatchDev bt, int 
 // sweep, q += dq), then the wall conditions of ImplicitAndUpdateVX.F90:76-77
 // and ImplicitAndUpdateTemp.F90:69-73.  One thread per column.
 // ---------------------------------------------------------------------------
+constexpr int K2_U = 4;   // planes loaded per chunk (loads of a chunk are all in flight together)
+
 __global__ void __launch_bounds__(256) k_implicit_bwd(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
@@ -399,84 +463,157 @@ __global__ void __launch_bounds__(256) k_implicit_bwd(BatchDev bt, int ns) {
   if (col >= B.plane) return;
   const int nx = B.nx, nxm = B.nxm;
   const long long P = B.plane;
-  const double *dX = coefp(B, SYS_X, C_DP), *uX = coefp(B, SYS_X, C_DU);
-  const double *dY = coefp(B, SYS_YZ, C_DP), *uY = coefp(B, SYS_YZ, C_DU);
-  const double *dT = coefp(B, SYS_T, C_DP), *uT = coefp(B, SYS_T, C_DU), *gT = coefp(B, SYS_T, C_G);
+  const double *__restrict__ dX = coefp(B, SYS_X, C_DP);
+  const double *__restrict__ uX = coefp(B, SYS_X, C_DU);
+  const double *__restrict__ dY = coefp(B, SYS_YZ, C_DP);
+  const double *__restrict__ uY = coefp(B, SYS_YZ, C_DU);
+  const double *__restrict__ dT = coefp(B, SYS_T, C_DP);
+  const double *__restrict__ uT = coefp(B, SYS_T, C_DU);
+  const double *__restrict__ gT = coefp(B, SYS_T, C_G);
+  const double *__restrict__ y0 = B.ybuf[0] + col;
+  const double *__restrict__ y1 = B.ybuf[1] + col;
+  const double *__restrict__ y2 = B.ybuf[2] + col;
+  const double *__restrict__ y3 = B.ybuf[3] + col;
+  double *__restrict__ vx = B.vx + col;
+  double *__restrict__ vy = B.vy + col;
+  double *__restrict__ vz = B.vz + col;
+  double *__restrict__ tp = B.temp + col;
   double xX = 0.0, xY = 0.0, xZ = 0.0;
-  for (int k = nxm - 1; k >= 0; --k) {
-    const long long o = (long long)k * P + col;
-    const double dy_ = __ldg(dY + k);
-    if (k == nxm - 1) {
-      xY = B.ybuf[1][o] / dy_;
-      xZ = B.ybuf[2][o] / dy_;
-    } else {
-      const double u = __ldg(uY + k);
-      xY = (B.ybuf[1][o] - u * xY) / dy_;
-      xZ = (B.ybuf[2][o] - u * xZ) / dy_;
+  // sweep 1: vx (rows nxm-1..1 of size nx), vy and vz (rows nxm-1..0 of size nxm)
+  for (int k0 = nxm - 1; k0 >= 0; k0 -= K2_U) {
+    double a0[K2_U], a1[K2_U], a2[K2_U], q0[K2_U], q1[K2_U], q2[K2_U];
+#pragma unroll
+    for (int u = 0; u < K2_U; ++u) {
+      const int k = k0 - u;
+      if (k >= 0) {
+        const long long o = (long long)k * P;
+        a1[u] = y1[o]; a2[u] = y2[o]; q1[u] = vy[o]; q2[u] = vz[o];
+        if (k >= 1) { a0[u] = y0[o]; q0[u] = vx[o]; }
+      }
     }
-    B.vy[o] = B.vy[o] + xY;
-    B.vz[o] = B.vz[o] + xZ;
-    if (k >= 1) {
-      xX = (B.ybuf[0][o] - __ldg(uX + k) * xX) / __ldg(dX + k);
-      B.vx[o] = B.vx[o] + xX;
+#pragma unroll
+    for (int u = 0; u < K2_U; ++u) {
+      const int k = k0 - u;
+      if (k < 0) break;
+      const long long o = (long long)k * P;
+      const double dy_ = __ldg(dY + k);
+      if (k == nxm - 1) {
+        xY = a1[u] / dy_;
+        xZ = a2[u] / dy_;
+      } else {
+        const double uu = __ldg(uY + k);
+        xY = (a1[u] - uu * xY) / dy_;
+        xZ = (a2[u] - uu * xZ) / dy_;
+      }
+      vy[o] = q1[u] + xY;
+      vz[o] = q2[u] + xZ;
+      if (k >= 1) {
+        xX = (a0[u] - __ldg(uX + k) * xX) / __ldg(dX + k);
+        vx[o] = q0[u] + xX;
+      }
     }
   }
-  B.vx[col] = 0.0;
-  B.vx[(long long)(nx - 1) * P + col] = 0.0;
+  vx[0] = 0.0;
+  vx[(long long)(nx - 1) * P] = 0.0;
   const double w = xZ;            // rhs(1,j,i) after the vz solve
   B.wall[col] = w;
+  // sweep 2: temperature, with the wall row's contribution g(k) * w
   double xT = 0.0;
-  for (int k = nxm - 1; k >= 1; --k) {
-    const long long o = (long long)k * P + col;
-    const double y = B.ybuf[3][o] + __ldg(gT + k) * w;
-    xT = (y - __ldg(uT + k) * xT) / __ldg(dT + k);
-    B.temp[o] = B.temp[o] + xT;
+  for (int k0 = nxm - 1; k0 >= 1; k0 -= K2_U) {
+    double a3[K2_U], q3[K2_U];
+#pragma unroll
+    for (int u = 0; u < K2_U; ++u) {
+      const int k = k0 - u;
+      if (k >= 1) { const long long o = (long long)k * P; a3[u] = y3[o]; q3[u] = tp[o]; }
+    }
+#pragma unroll
+    for (int u = 0; u < K2_U; ++u) {
+      const int k = k0 - u;
+      if (k < 1) break;
+      const double y = a3[u] + __ldg(gT + k) * w;
+      xT = (y - __ldg(uT + k) * xT) / __ldg(dT + k);
+      tp[(long long)k * P] = q3[u] + xT;
+    }
   }
-  B.temp[col] = B.tempbp;
-  B.temp[(long long)(nx - 1) * P + col] = B.temptp;
+  tp[0] = B.tempbp;
+  tp[(long long)(nx - 1) * P] = B.temptp;
 }
 
 // ---------------------------------------------------------------------------
 // Projection: CorrectVelocity.F90:19-44 and CorrectPressure.F90:19-51 in one
 // pass over the cells k = 1..nxm.  Thread per cell.
 // ---------------------------------------------------------------------------
+constexpr int KC_U = 4;   // planes per prefetch chunk
+
 __global__ void __launch_bounds__(256) k_correct(BatchDev bt, int ns, int do_vel, int do_pr) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
   const BoxScalars *S = B.sc;
   if (S->status != 0) return;
-  const long long cell = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
+  const long long col = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
   const long long P = B.plane;
-  if (cell >= (long long)B.nxm * P) return;
-  const int k = (int)(cell / P);
-  const long long col = cell - (long long)k * P;
-  const int i = (int)(col / B.nym);
-  const int j = (int)(col - (long long)i * B.nym);
-  const int nym = B.nym, nzm = B.nzm;
+  if (col >= P) return;
+  const int nym = B.nym, nzm = B.nzm, nxm = B.nxm;
+  const int i = (int)(col / nym);
+  const int j = (int)(col - (long long)i * nym);
   const int im = i == 0 ? nzm - 1 : i - 1, ip = i == nzm - 1 ? 0 : i + 1;
   const int jm = j == 0 ? nym - 1 : j - 1, jp = j == nym - 1 ? 0 : j + 1;
-  const int km = k == 0 ? 0 : k - 1;                 // kmv
-  const int kp = k == B.nxm - 1 ? k : k + 1;         // kpv
-  const double *phi = B.phi;
-  const double f = phi[cell];
+  const long long oim = (long long)im * nym + j - col, oip = (long long)ip * nym + j - col;
+  const long long ojm = (long long)i * nym + jm - col, ojp = (long long)i * nym + jp - col;
+  const double *__restrict__ phi = B.phi + col;
+  double *__restrict__ vx = B.vx + col;
+  double *__restrict__ vy = B.vy + col;
+  double *__restrict__ vz = B.vz + col;
+  double *__restrict__ pr = B.pr + col;
   const double al = S->al, dt = S->dt;
-  if (do_vel) {
-    const double udy = al * dt * B.dy;
-    const double udz = al * dt * B.dz;
-    const double usukm = al * dt * tabk(B, T_UDX3C, k);
-    if (k >= 1) B.vx[cell] = B.vx[cell] - (f - phi[(long long)km * P + col]) * usukm;
-    B.vy[cell] = B.vy[cell] - (f - phi[(long long)k * P + (long long)i * nym + jm]) * udy;
-    B.vz[cell] = B.vz[cell] - (f - phi[(long long)k * P + (long long)im * nym + j]) * udz;
-  }
-  if (do_pr) {
-    const double be = al * S->beta;
-    const double amm = tabk(B, T_AMPHK, k), acc = tabk(B, T_ACPHK, k), app = tabk(B, T_APPHK, k);
-    const long long pk = (long long)k * P;
-    const double zz = (phi[pk + (long long)ip * nym + j] - 2.0 * f + phi[pk + (long long)im * nym + j]) * B.dzq;
-    const double yy = (phi[pk + (long long)i * nym + jp] - 2.0 * f + phi[pk + (long long)i * nym + jm]) * B.dyq;
-    const double xx = phi[(long long)kp * P + col] * app + f * acc + phi[(long long)km * P + col] * amm;
-    B.pr[cell] = B.pr[cell] + f - be * (zz + yy + xx);
+  const double udy = al * dt * B.dy;
+  const double udz = al * dt * B.dz;
+  const double be = al * S->beta;
+  const double dzq = B.dzq, dyq = B.dyq;
+  double fm = phi[0];          // phi(kmv(k)) for k = 0 is phi(0)
+  double fc = fm;
+  for (int k0 = 0; k0 < nxm; k0 += KC_U) {
+    double fn[KC_U], fzp[KC_U], fzm[KC_U], fyp[KC_U], fym[KC_U];
+    double qx[KC_U], qy[KC_U], qz[KC_U], qp[KC_U];
+#pragma unroll
+    for (int u = 0; u < KC_U; ++u) {
+      const int k = k0 + u;
+      if (k < nxm) {
+        const long long o = (long long)k * P;
+        const int kn = k + 1 < nxm ? k + 1 : k;     // kpv
+        fn[u] = phi[(long long)kn * P];
+        fzp[u] = phi[o + oip]; fzm[u] = phi[o + oim];
+        fyp[u] = phi[o + ojp]; fym[u] = phi[o + ojm];
+        if (do_vel) { qx[u] = vx[o]; qy[u] = vy[o]; qz[u] = vz[o]; }
+        if (do_pr) qp[u] = pr[o];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < KC_U; ++u) {
+      const int k = k0 + u;
+      if (k >= nxm) break;
+      const long long o = (long long)k * P;
+      const double f = fc;
+      if (do_vel) {
+        // CorrectVelocity.F90:32-41
+        const double usukm = al * dt * tabk(B, T_UDX3C, k);
+        if (k >= 1) vx[o] = qx[u] - (f - fm) * usukm;
+        vy[o] = qy[u] - (f - fym[u]) * udy;
+        vz[o] = qz[u] - (f - fzm[u]) * udz;
+      }
+      if (do_pr) {
+        // CorrectPressure.F90:33-48 (kpv/kmv clamp at the walls)
+        const double amm = tabk(B, T_AMPHK, k), acc = tabk(B, T_ACPHK, k), app = tabk(B, T_APPHK, k);
+        const double fkm = k == 0 ? f : fm;
+        const double zz = (fzp[u] - 2.0 * f + fzm[u]) * dzq;
+        const double yy = (fyp[u] - 2.0 * f + fym[u]) * dyq;
+        const double xx = fn[u] * app + f * acc + fkm * amm;
+        pr[o] = qp[u] + f - be * (zz + yy + xx);
+      }
+      fm = f;
+      fc = fn[u];
+    }
   }
 }
 

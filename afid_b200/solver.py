@@ -108,6 +108,15 @@ class Context:
         f = self._L.afid_step_graph if graph else self._L.afid_step
         _lib.check(f(self.h, ids, n, nsteps))
 
+    def step_profiled(self, boxes, nsteps: int = 1) -> dict:
+        """Per-kernel device time (ms, summed over nsteps) and launch counts."""
+        ids, n = self._ids(boxes)
+        nk = len(_lib.KERNELS)
+        ms = (C.c_double * nk)()
+        cnt = (C.c_int * nk)()
+        _lib.check(self._L.afid_step_profiled(self.h, ids, n, nsteps, ms, cnt, nk))
+        return {k: (ms[q], cnt[q]) for q, k in enumerate(_lib.KERNELS)}
+
     def substep(self, boxes, ns: int):
         ids, n = self._ids(boxes)
         _lib.check(self._L.afid_substep(self.h, ids, n, ns))

@@ -156,6 +156,28 @@ int afid_step_graph(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
 /* One substep ns of TimeMarcher.F90:28-72 with the current dt (no CFL). */
 int afid_substep(afid_ctx *ctx, const int *box_ids, int nbox, int ns);
 
+/* Kernel slots of afid_step_profiled. */
+enum afid_kernel {
+  AFID_K_DIAG = 0,          /* CalcMaxCFL + CheckDivergence + vmax reduction */
+  AFID_K_FINALIZE = 1,      /* dt rule / step bookkeeping */
+  AFID_K_PREP = 2,          /* substep coefficients and x-tridiagonal LU */
+  AFID_K_EXPLICIT_FWD = 3,  /* ExplicitTerms* + ImplicitAndUpdate* rhs + forward sweeps */
+  AFID_K_IMPLICIT_BWD = 4,  /* back substitution + update of vx, vy, vz, temp */
+  AFID_K_FFT_Y_FWD = 5,     /* CalcLocalDivergence + r2c along y */
+  AFID_K_FFT_Z_FWD = 6,     /* c2c along z, forward */
+  AFID_K_POISSON_X = 7,     /* complex tridiagonal per (ky, kz) */
+  AFID_K_FFT_Z_INV = 8,     /* c2c along z, backward */
+  AFID_K_FFT_Y_INV = 9,     /* c2r along y into dph */
+  AFID_K_CORRECT = 10,      /* CorrectVelocity + CorrectPressure */
+  AFID_K_PLATE_NU = 11,     /* CalcPlateNu partial sums */
+  AFID_K_COUNT = 12
+};
+/* afid_step with a CUDA event after every launch: adds each kernel's
+ * device time (ms) into kernel_ms[slot] and its launch count into
+ * kernel_launches[slot] (may be NULL); nkernel >= AFID_K_COUNT. */
+int afid_step_profiled(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps,
+                       double *kernel_ms, int *kernel_launches, int nkernel);
+
 #ifdef __cplusplus
 }
 #endif

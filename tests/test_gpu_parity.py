@@ -1,0 +1,165 @@
+"""The fused step (afid_step) against the oracle on seeded inputs.
+
+Tolerances (from the parity contract): per-field relative L2 <= 1e-11 after
+one step, pr compared after removing its volume mean (the singular (0,0)
+Poisson mode fixes pr only up to a constant); max divergence <= 1e-10 every
+step; plate Nusselt numbers to 1e-9."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import cfg_of, compare_fields, oracle_state, FIELDS
+from oracle import afid_oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _box(ctx, cfg, s):
+    box = ctx.add_box(cfg, s.g.xc)
+    for f in FIELDS:
+        box.upload(f, getattr(s, f))
+    return box
+
+
+@pytest.mark.parametrize("shape,kw", [
+    ((24, 16, 12), dict(ray=1e5, pra=0.7, zlen=0.75)),
+    ((32, 48, 32), dict(ray=1e7, pra=1.0, ylen=1.5)),
+    ((20, 20, 40), dict(ray=3e6, pra=4.38, ylen=1.0, zlen=2.0)),
+    ((16, 32, 16), dict(ray=1e6, inslws=0, inslwn=0, istr3=6, str3=2.0)),
+])
+def test_fused_step_matches_oracle(ctx, shape, kw):
+    cfg = cfg_of(*shape, dt=5e-4, **kw)
+    s = oracle_state(cfg, seed=1)
+    box = _box(ctx, cfg, s)
+    recs = O.run(s, 1, cfg.dt)
+    ctx.step([box], 1)
+    err = compare_fields(box, s)
+    assert all(v <= 1e-11 for v in err.values()), err
+    sc = box.scalars()
+    assert sc["status"] == 0 and sc["ntime"] == 1
+    assert abs(sc["nu_bot"] - recs[0]["nu_bot"]) <= 1e-9
+    assert abs(sc["nu_top"] - recs[0]["nu_top"]) <= 1e-9
+    ctx.remove_box(box)
+
+
+def test_c1_one_step_and_divergence_every_step(ctx):
+    cfg = cfg_of(64, 64, 64, ray=1e6, dt=5e-4)
+    s = oracle_state(cfg, seed=0)
+    box = _box(ctx, cfg, s)
+    O.run(s, 1, cfg.dt, vectorised_poisson=True)
+    ctx.step([box], 1)
+    err = compare_fields(box, s)
+    assert all(v <= 1e-11 for v in err.values()), err
+    for _ in range(5):
+        ctx.step([box], 1)
+        assert box.check_divergence() <= 1e-10
+    ctx.remove_box(box)
+
+
+def test_c1_plate_nu_100_steps_against_golden(ctx):
+    z = np.load(os.path.join(GOLDEN, "golden_c1_nu.npz"))
+    cfg = cfg_of(64, 64, 64, ray=1e6, dt=5e-4)
+    s = oracle_state(cfg, seed=0)
+    box = _box(ctx, cfg, s)
+    ctx.step([box], 100, graph=True)
+    hist = box.history()
+    assert len(hist) == 100
+    nb = np.array([h["nu_bot"] for h in hist])
+    nt = np.array([h["nu_top"] for h in hist])
+    assert np.abs(nb - z["nu_bot"]).max() <= 1e-9
+    assert np.abs(nt - z["nu_top"]).max() <= 1e-9
+    assert np.allclose([h["dt"] for h in hist], z["dt"], rtol=0, atol=0)
+    for f in FIELDS:
+        a = box.download(f)
+        if f == "pr":
+            a = a[:-1] - a[:-1].mean()
+        ref = z[f"sum_{f}"]
+        assert abs((a * a).sum() - ref[1]) <= 1e-9 * max(abs(ref[1]), 1e-30), f
+    assert box.check_divergence() <= 1e-10
+    ctx.remove_box(box)
+
+
+def test_golden_small_five_steps(ctx):
+    z = np.load(os.path.join(GOLDEN, "golden_small.npz"))
+    cfg = cfg_of(24, 16, 12, ray=1e5, pra=0.7, zlen=0.75, dt=5e-4)
+    s = oracle_state(cfg, seed=11)
+    box = _box(ctx, cfg, s)
+    ctx.step([box], 1)
+    for f in FIELDS:
+        d, g = box.download(f), z[f"step1_{f}"]
+        if f == "pr":
+            d, g = d[:-1] - d[:-1].mean(), g[:-1] - g[:-1].mean()
+        assert np.linalg.norm(d - g) <= 1e-11 * max(np.linalg.norm(g), 1e-30), f
+    ctx.step([box], 4)
+    for f in FIELDS:
+        d, g = box.download(f), z[f"step5_{f}"]
+        if f == "pr":
+            d, g = d[:-1] - d[:-1].mean(), g[:-1] - g[:-1].mean()
+        assert np.linalg.norm(d - g) <= 1e-10 * max(np.linalg.norm(g), 1e-30), f
+    hist = box.history()
+    assert np.abs(np.array([h["nu_bot"] for h in hist]) - z["nu_bot"]).max() <= 1e-9
+    ctx.remove_box(box)
+
+
+def test_conduction_fixed_point_on_gpu(ctx):
+    cfg = cfg_of(48, 32, 24, ray=1e7, zlen=0.75)
+    s = oracle_state(cfg, seed=None)
+    box = _box(ctx, cfg, s)
+    ctx.step([box], 3)
+    assert np.abs(box.download("temp") - s.temp).max() <= 1e-14
+    for f in ("vx", "vy", "vz"):
+        assert np.abs(box.download(f)).max() < 1e-18
+    sc = box.scalars()
+    assert sc["nu_bot"] == pytest.approx(1.0, abs=1e-13)
+    assert sc["nu_top"] == pytest.approx(1.0, abs=1e-13)
+    ctx.remove_box(box)
+
+
+def test_adams_bashforth_variant(ctx):
+    cfg = cfg_of(24, 16, 12, ray=1e5, zlen=0.75, dt=2e-4, nsst=1)
+    s = oracle_state(cfg, seed=2)
+    box = _box(ctx, cfg, s)
+    O.run(s, 3, cfg.dt)
+    ctx.step([box], 3)
+    err = compare_fields(box, s)
+    assert all(v <= 1e-11 for v in err.values()), err
+    ctx.remove_box(box)
+
+
+def test_adaptive_dt_follows_reference_rule(ctx):
+    cfg = cfg_of(24, 16, 12, ray=1e6, zlen=0.75, dt=1e-3, idtv=1, cflmax=1.2, dtmin=1e-5, dtmax=2e-3)
+    s = oracle_state(cfg, seed=6)
+    box = _box(ctx, cfg, s)
+    recs = O.run(s, 4, cfg.dt, idtv=1, cflmax=1.2, dtmin=1e-5, dtmax=2e-3)
+    ctx.step([box], 4)
+    hist = box.history()
+    assert [h["dt"] for h in hist] == pytest.approx([r["dt"] for r in recs], rel=1e-12)
+    err = compare_fields(box, s)
+    assert all(v <= 1e-10 for v in err.values()), err
+    ctx.remove_box(box)
+
+
+def test_full_size_box_properties(ctx):
+    """The large-box configuration (385 x 768 x 768): conduction stays a
+    fixed point and a seeded step keeps the divergence at roundoff."""
+    cfg = cfg_of(384, 768, 768, ray=1e9, ylen=2.0, zlen=2.0, dt=1e-4)
+    s_small = O.init_state(O.Params(nxm=384, nym=2, nzm=2), seed=None, ic="conduction")
+    xc = s_small.g.xc
+    from afid_b200.ic import initial_fields
+    box = ctx.add_box(cfg, xc)
+    f = initial_fields(cfg, xc, seed=None)
+    for k, v in f.items():
+        box.upload(k, v)
+    ctx.step([box], 1)
+    t = box.download("temp")
+    assert np.abs(t - f["temp"]).max() <= 1e-14
+    f = initial_fields(cfg, xc, seed=0)
+    for k, v in f.items():
+        box.upload(k, v)
+    box.reset()
+    ctx.step([box], 2)
+    assert box.check_divergence() <= 1e-10
+    assert box.scalars()["status"] == 0
+    ctx.remove_box(box)
