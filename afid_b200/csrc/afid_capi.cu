@@ -1014,3 +1014,177 @@ int afid_step_graph(afid_ctx *c, const int *ids, int n, int nsteps) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Pressure solve without allocation.
+//
+// For callers that cannot allocate device memory at run time -- an
+// application that hands all GPU memory to its own pool before it calls us,
+// code that runs where cudaMalloc is not allowed, or a host program that
+// keeps its fields on the device and must not grow its footprint per call --
+// this entry point runs the same five pressure-solve kernels as
+// afid_solve_pressure_correction, but keeps its scratch (half spectrum,
+// Thomas pivots, metric tables, twiddles and kernel descriptors) in one
+// file-scope device array instead of a box.  The caller passes only dph.
+//
+// The array is fixed at AFID_NOALLOC_DOUBLES doubles (about 48.5 MiB) and
+// every GPU on which the library is loaded holds it until the process exits.
+// Every call shares it and it keeps the previous call's contents; each call
+// rewrites everything it reads, so nothing has to start at zero.  Calls
+// whose work overlaps on the GPU (two streams, or two host threads) race on
+// it and must be serialised by the caller.
+// ============================================================================
+namespace {
+
+constexpr long long NOALLOC_MAX_SPEC = 1LL << 21;            // nxm * nzm * (nym/2 + 1)
+constexpr int NOALLOC_MAX_NXM = 1024;
+constexpr int NOALLOC_MAX_NYZ = 4096;
+constexpr long long NOALLOC_META = 1LL << 16;                // tables, twiddles, descriptors
+constexpr long long AFID_NOALLOC_DOUBLES = 3 * NOALLOC_MAX_SPEC + NOALLOC_META;
+
+static __device__ __align__(256) double g_noalloc_scratch[AFID_NOALLOC_DOUBLES];
+
+// device address of g_noalloc_scratch per device (host code may not use the
+// symbol itself as an address)
+double *g_noalloc_base[64] = {};
+
+int noalloc_setup(int dev) {
+  if (dev < 0 || dev >= 64) return fail(AFID_EINVAL, "noalloc: device %d out of range", dev);
+  if (g_noalloc_base[dev]) return 0;
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(AFID_ECUDA, "noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+  g_noalloc_base[dev] = (double *)p;
+  return 0;
+}
+
+// host staging of the small per-call data (no heap allocation per call)
+struct NoallocHost {
+  double tab[(size_t)T_NK * (NOALLOC_MAX_NXM + 1) + 2 * NOALLOC_MAX_NYZ];
+  double2 tw[2 * NOALLOC_MAX_NYZ];
+};
+NoallocHost g_noalloc_host;
+
+}  // namespace
+
+extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int nym, int nzm,
+                                                      const double *xc, double alx3, double ylen,
+                                                      double zlen, void *stream) {
+  if (!dph || !xc) return fail(AFID_EINVAL, "noalloc: dph and xc are required");
+  if (nxm < 3 || nym < 2 || nzm < 2 || (nym % 2))
+    return fail(AFID_EINVAL, "noalloc: need nxm >= 3, nzm >= 2 and an even nym >= 2");
+  if (!(alx3 > 0) || !(ylen > 0) || !(zlen > 0)) return fail(AFID_EINVAL, "noalloc: lengths must be > 0");
+  const long long nspec = (long long)nxm * nzm * (nym / 2 + 1);
+  if (nxm > NOALLOC_MAX_NXM || nym > NOALLOC_MAX_NYZ || nzm > NOALLOC_MAX_NYZ || nspec > NOALLOC_MAX_SPEC)
+    return fail(AFID_ESIZE,
+                "noalloc: box %dx%dx%d exceeds the fixed scratch: nxm <= %d, nym, nzm <= %d and "
+                "nxm*nzm*(nym/2+1) <= %lld (got %lld)",
+                nxm, nym, nzm, NOALLOC_MAX_NXM, NOALLOC_MAX_NYZ, NOALLOC_MAX_SPEC, nspec);
+  for (int k = 1; k <= nxm; ++k)
+    if (!(xc[k] > xc[k - 1])) return fail(AFID_EINVAL, "noalloc: xc must be increasing");
+  BoxDev d;
+  memset(&d, 0, sizeof d);
+  if (factor_radices(nym, d.fft_y_radix, &d.fft_y_np) || factor_radices(nzm, d.fft_z_radix, &d.fft_z_np))
+    return fail(AFID_EFFT, "noalloc: nym=%d nzm=%d need prime factors <= 7", nym, nzm);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  int rc = noalloc_setup(dev);
+  if (rc) return rc;
+  rc = init_kernel_attrs();
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  double *base = g_noalloc_base[dev];
+
+  // device layout of the scratch array (offsets in doubles)
+  const int nx = nxm + 1;
+  const long long o_spec = 0, o_dstore = 2 * NOALLOC_MAX_SPEC, o_meta = 3 * NOALLOC_MAX_SPEC;
+  const long long n_tab = (long long)T_NK * nx + nzm + nym;
+  const long long o_tab = o_meta;
+  const long long o_tw = (o_tab + n_tab + 1) & ~1LL;
+  const long long o_sc = (o_tw + 2LL * (nym + nzm) + 7) & ~7LL;
+  const long long o_box = o_sc + (long long)((sizeof(BoxScalars) + 63) / 8);
+  const long long o_off = o_box + (long long)((sizeof(BoxDev) + 63) / 8);
+  if (o_off + 16 > AFID_NOALLOC_DOUBLES) return fail(AFID_ESIZE, "noalloc: tables do not fit");
+
+  // tables: the Poisson rows of InitPressureSolver.F90:22-59 (other k-tables unused)
+  double *tab = g_noalloc_host.tab;
+  for (long long q = 0; q < n_tab; ++q) tab[q] = 0.0;
+  {
+    const double pi = 2.0 * std::asin(1.0);
+    const double dx = (double)nxm / alx3, dxq = dx * dx;
+    auto g3rm = [&](int kc) { return (xc[kc] - xc[kc - 1]) * dx; };               // kc 1-based
+    auto g3rc = [&](int kc) {
+      if (kc == 1) return (xc[1] - xc[0]) * dx;
+      if (kc == nx) return (xc[nx - 1] - xc[nxm - 1]) * dx;
+      return (xc[kc] - xc[kc - 2]) * dx * 0.5;
+    };
+    for (int kc = 1; kc <= nxm; ++kc) {
+      const int kp = (kc == nxm) ? kc : kc + 1;
+      const double kmc = (kc == 1) ? 0.0 : 1.0, kpc = (kc == nxm) ? 0.0 : 1.0;
+      const double a33icc = kmc * dxq / g3rc(kc);
+      const double a33icp = kpc * dxq / g3rc(kp);
+      const double ugmmm = 1.0 / g3rm(kc);
+      tab[(size_t)T_AMPHK * nx + kc - 1] = a33icc * ugmmm;
+      tab[(size_t)T_APPHK * nx + kc - 1] = a33icp * ugmmm;
+      tab[(size_t)T_ACPHK * nx + kc - 1] = -(a33icc * ugmmm + a33icp * ugmmm);
+    }
+    double *ak1 = tab + (size_t)T_NK * nx, *ak2 = ak1 + nzm;
+    const int nzmh = nzm / 2 + 1, nymh = nym / 2 + 1;
+    for (int i = 1; i <= nzm; ++i) {
+      const double ao = (i <= nzmh) ? (i - 1) * 2.0 * pi : -(nzm - i + 1) * 2.0 * pi;
+      const double f = (double)nzm / zlen;
+      ak1[i - 1] = 2.0 * (1.0 - std::cos(ao / nzm)) * (f * f);
+    }
+    for (int j = 1; j <= nym; ++j) {
+      const double ap = (j <= nymh) ? (j - 1) * 2.0 * pi : -(nym - j + 1) * 2.0 * pi;
+      const double f = (double)nym / ylen;
+      ak2[j - 1] = 2.0 * (1.0 - std::cos(ap / nym)) * (f * f);
+    }
+  }
+  build_twiddles(nym, g_noalloc_host.tw);
+  build_twiddles(nzm, g_noalloc_host.tw + nym);
+
+  // descriptor of a one-box batch pointing into the scratch array; dph is
+  // both the input (phi) and the output of the solve
+  d.nxm = nxm; d.nx = nx; d.nym = nym; d.nzm = nzm; d.nymh = nym / 2 + 1;
+  d.nsst = 1;
+  d.plane = (long long)nym * nzm;
+  d.fsize = (long long)nx * d.plane;
+  d.nspec = nspec;
+  d.phi = dph;
+  d.spec = (double2 *)(base + o_spec);
+  d.dstore = base + o_dstore;
+  d.tab = base + o_tab;
+  d.twy = (const double2 *)(base + o_tw);
+  d.twz = (const double2 *)(base + o_tw) + nym;
+  d.sc = (BoxScalars *)(base + o_sc);
+  d.active = 1;
+  BoxScalars bs;
+  memset(&bs, 0, sizeof bs);
+  int off[3][2];
+  off[0][0] = 0; off[0][1] = (int)tiles_of(d, FAM_FY);
+  off[1][0] = 0; off[1][1] = (int)tiles_of(d, FAM_FZ);
+  off[2][0] = 0; off[2][1] = (int)tiles_of(d, FAM_PX);
+  CK(cudaMemcpyAsync(base + o_tab, tab, (size_t)n_tab * 8, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_tw, g_noalloc_host.tw, (size_t)(nym + nzm) * 16, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_box, &d, sizeof d, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_off, off, sizeof off, cudaMemcpyHostToDevice, st));
+  const BoxDev *dbox = (const BoxDev *)(base + o_box);
+  const int *doff = (const int *)(base + o_off);
+  BatchDev fy{dbox, doff + 0, 1}, fz{dbox, doff + 2, 1}, px{dbox, doff + 4, 1};
+  const size_t sy = (size_t)fft_smem_bytes(nym, fft_y_pairs(nym));
+  const size_t sz = (size_t)fft_smem_bytes(nzm, fft_z_lines(nzm));
+  k_fft_y_fwd<false><<<off[0][1], FFT_T, sy, st>>>(fy, 0);
+  CKL();
+  k_fft_z<<<off[1][1], FFT_T, sz, st>>>(fz, 0, -1);
+  CKL();
+  k_poisson_x<<<off[2][1], 256, 0, st>>>(px, 0);
+  CKL();
+  k_fft_z<<<off[1][1], FFT_T, sz, st>>>(fz, 0, +1);
+  CKL();
+  k_fft_y_inv<<<off[0][1], FFT_T, sy, st>>>(fy, 0);
+  CKL();
+  return 0;
+}

@@ -178,6 +178,28 @@ enum afid_kernel {
 int afid_step_profiled(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps,
                        double *kernel_ms, int *kernel_launches, int nkernel);
 
+/* ---- pressure solve without allocation ------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they run (memory handed to their own pool, code paths where
+ * cudaMalloc is not allowed, a fixed device footprint): the pressure solve of
+ * afid_solve_pressure_correction on a dph array the caller owns, with all
+ * scratch in one fixed device array inside the library (about 48.5 MiB, held
+ * on every GPU that loads the library until exit).  No cudaMalloc, cudaFree or
+ * other allocating call is made.
+ *   dph    device pointer, in/out: nxm*nym*nzm doubles in the library's
+ *          device layout dph[k][i][j] (y fastest, then z, then x)
+ *   xc     host pointer: the nx = nxm+1 node positions
+ *   stream cudaStream_t to queue the work on (0: the default stream)
+ * Limits: nxm <= 1024, nym and nzm <= 4096 (nym even, prime factors <= 7),
+ * nxm*nzm*(nym/2+1) <= 2^21; larger boxes return AFID_ESIZE.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array and find
+ * the previous call's contents in it; calls that overlap on the GPU race, so
+ * the caller must not run two at once.  Returns after queueing the work. */
+int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int nym, int nzm,
+                                           const double *xc, double alx3, double ylen,
+                                           double zlen, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
