@@ -7,32 +7,88 @@
 // The 2DECOMP pencil transposes of the reference disappear: each transform
 // reads its lines directly from the plane-major layout.
 //
-// The FFTs are Stockham auto-sort passes of radix 4, 2, 3, 5 and 7 in shared
-// memory, ping-ponging between two buffers.  Twiddles exp(-2 pi i n / N) come
-// from a table computed on the host in extended precision and copied to
-// shared memory by every block.
+// The FFTs are Stockham auto-sort passes of radix 16, 8, 4, 2, 3, 5 and 7
+// (plans in increasing radix order, e.g. 768 = 3 x 16 x 16): the first pass
+// streams from global memory, the inner passes run in place in shared memory
+// and the last pass of the z and inverse-y transforms streams back to global
+// memory.  Twiddles exp(-2 pi i n / N) come from a table computed on the host
+// in extended precision and copied to shared memory by every block.
 #pragma once
 #include "afid_device.cuh"
 
 namespace afid {
 
 // radix-R butterfly on v[0..R-1] (unnormalised DFT, exponent sign ``sgn``)
+__device__ __forceinline__ double2 cmul_wi(double2 a, double c, double s, int sgn) {
+  // a * (c + i sgn s)
+  const double ss = sgn > 0 ? s : -s;
+  return make_double2(a.x * c - a.y * ss, a.x * ss + a.y * c);
+}
+__device__ __forceinline__ double2 mul_sgn_i(double2 a, int sgn) {   // a * (sgn i)
+  return make_double2(-sgn * a.y, sgn * a.x);
+}
+__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, double2 &a3, int sgn) {
+  const double2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
+  const double2 t2 = cadd(a1, a3), t3 = csub(a1, a3);
+  const double2 wt3 = mul_sgn_i(t3, sgn);
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, wt3);
+  a3 = csub(t1, wt3);
+}
+
 template <int R>
 __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double2 *tw, int N) {
-  if (R == 2) {
+  constexpr double H = 0.70710678118654752440;    // cos(pi/4)
+  constexpr double C8 = 0.92387953251128675613;   // cos(pi/8)
+  constexpr double S8 = 0.38268343236508977173;   // sin(pi/8)
+  if constexpr (R == 2) {
     const double2 a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
-  } else if (R == 4) {
-    const double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-    const double2 t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
-    // w * t3 with w = sgn * i
-    const double2 wt3 = make_double2(-sgn * t3.y, sgn * t3.x);
-    v[0] = cadd(t0, t2);
-    v[2] = csub(t0, t2);
-    v[1] = cadd(t1, wt3);
-    v[3] = csub(t1, wt3);
-  } else if (R == 3) {
+  } else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3], sgn);
+  } else if constexpr (R == 8) {
+    // 8 = 2 x 4: four-point DFTs over n2 of x[n1 + 2 n2], twiddle W8^(n1 k2),
+    // two-point DFTs over n1; X[4 k1 + k2]
+    double2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
+    double2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
+    dft4(a0, a1, a2, a3, sgn);
+    dft4(b0, b1, b2, b3, sgn);
+    b1 = cmul_wi(b1, H, H, sgn);
+    b2 = mul_sgn_i(b2, sgn);
+    b3 = cmul_wi(b3, -H, H, sgn);
+    v[0] = cadd(a0, b0); v[4] = csub(a0, b0);
+    v[1] = cadd(a1, b1); v[5] = csub(a1, b1);
+    v[2] = cadd(a2, b2); v[6] = csub(a2, b2);
+    v[3] = cadd(a3, b3); v[7] = csub(a3, b3);
+  } else if constexpr (R == 16) {
+    // 16 = 4 x 4: four-point DFTs over n2 of x[n1 + 4 n2] (results Y[n1][k2]
+    // kept in v[n1 + 4 k2]), twiddle by W16^(n1 k2), four-point DFTs over n1
+    // (X[4 k1 + k2] lands in v[4 k2 + k1]), then a register renaming into
+    // natural order.
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) dft4(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12], sgn);
+    v[5] = cmul_wi(v[5], C8, S8, sgn);        // n1=1 k2=1: m=1
+    v[9] = cmul_wi(v[9], H, H, sgn);          // n1=1 k2=2: m=2
+    v[13] = cmul_wi(v[13], S8, C8, sgn);      // n1=1 k2=3: m=3
+    v[6] = cmul_wi(v[6], H, H, sgn);          // n1=2 k2=1: m=2
+    v[10] = mul_sgn_i(v[10], sgn);            // n1=2 k2=2: m=4
+    v[14] = cmul_wi(v[14], -H, H, sgn);       // n1=2 k2=3: m=6
+    v[7] = cmul_wi(v[7], S8, C8, sgn);        // n1=3 k2=1: m=3
+    v[11] = cmul_wi(v[11], -H, H, sgn);       // n1=3 k2=2: m=6
+    v[15] = cmul_wi(v[15], -C8, -S8, sgn);    // n1=3 k2=3: m=9
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) dft4(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3], sgn);
+    // X[4 k1 + k2] = v[4 k2 + k1]: transpose the 4 x 4 index grid
+    double2 t;
+    t = v[1]; v[1] = v[4]; v[4] = t;
+    t = v[2]; v[2] = v[8]; v[8] = t;
+    t = v[3]; v[3] = v[12]; v[12] = t;
+    t = v[6]; v[6] = v[9]; v[9] = t;
+    t = v[7]; v[7] = v[13]; v[13] = t;
+    t = v[11]; v[11] = v[14]; v[14] = t;
+  } else if constexpr (R == 3) {
     const double S3 = 0.86602540378443864676;   // sin(2 pi / 3)
     const double2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
     const double2 a0 = v[0];
@@ -41,7 +97,7 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
     v[0] = cadd(a0, s);
     v[1] = cadd(m, id);
     v[2] = csub(m, id);
-  } else if (R == 5) {
+  } else if constexpr (R == 5) {
     const double C1 = 0.30901699437494742410, C2 = -0.80901699437494742410;
     const double S1 = 0.95105651629515357212, S2 = 0.58778525229247312917;
     const double2 a0 = v[0];
@@ -51,9 +107,8 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
     const double2 r2 = make_double2(a0.x + C2 * s14.x + C1 * s23.x, a0.y + C2 * s14.y + C1 * s23.y);
     const double2 q1 = make_double2(S1 * d14.x + S2 * d23.x, S1 * d14.y + S2 * d23.y);
     const double2 q2 = make_double2(S2 * d14.x - S1 * d23.x, S2 * d14.y - S1 * d23.y);
-    // multiply by sgn * i
-    const double2 iq1 = make_double2(-sgn * q1.y, sgn * q1.x);
-    const double2 iq2 = make_double2(-sgn * q2.y, sgn * q2.x);
+    const double2 iq1 = mul_sgn_i(q1, sgn);
+    const double2 iq2 = mul_sgn_i(q2, sgn);
     v[0] = make_double2(a0.x + s14.x + s23.x, a0.y + s14.y + s23.y);
     v[1] = cadd(r1, iq1);
     v[4] = csub(r1, iq1);
@@ -79,91 +134,160 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
   }
 }
 
-// One Stockham pass of radix R over L lines of length N, from buffer a into
-// buffer b (both in shared memory).  LINE_MAJOR: element (l, n) at l*N + n,
-// else at n*L + l.
-constexpr int FFT_T = 256;          // threads per FFT block
-constexpr int FFT_ELEMS = 3072;     // lines x N per block (two buffers: 96 KB)
+// Stockham passes over L lines of length N.  Pass p with radix R reads
+// element j + r N/R of each butterfly j and writes element
+// (j / Ns) Ns R + j % Ns + r Ns, Ns being the product of the earlier radices.
+// Every pass streams from a source functor to a destination functor: the
+// first pass reads global memory, inner passes go between two shared
+// buffers, and the last pass of the z and inverse-y transforms writes global
+// memory.  LINE_MAJOR: element (l, n) at l*N + n, else at n*L + l.
+constexpr int FFT_T = 256;    // threads per FFT block
 
-template <int R, bool LINE_MAJOR>
-__device__ __forceinline__ void stockham_pass(const double2 *__restrict__ a, double2 *__restrict__ b,
-                                              int N, int L, int Ns, int sgn, const double2 *tw) {
-  const int NR = N / R;
-  const int tstr = N / (Ns * R);
-  const int total = NR * L;
+template <bool LM>
+__device__ __forceinline__ void bfly_index(int t, int NR, int L, int &l, int &j) {
+  if (LM) { j = t % NR; l = t / NR; } else { l = t % L; j = t / L; }
+}
+template <bool LM>
+__device__ __forceinline__ int sidx(int l, int n, int N, int L) { return LM ? l * N + n : n * L + l; }
+
+template <int R>
+__device__ __forceinline__ void twiddle(double2 (&v)[R], int k, int tstr, int sgn, const double2 *tw) {
+#pragma unroll
+  for (int r = 1; r < R; ++r) {
+    double2 w = tw[r * k * tstr];
+    if (sgn > 0) w.y = -w.y;
+    v[r] = cmul(v[r], w);
+  }
+}
+
+template <int R, bool LM, class Src, class Dst>
+__device__ __forceinline__ void pass_stream(int N, int L, int Ns, int sgn, const double2 *tw,
+                                            const Src &src, const Dst &dst) {
+  const int NR = N / R, tstr = N / (Ns * R), total = NR * L;
   for (int t = threadIdx.x; t < total; t += FFT_T) {
     int l, j;
-    if (LINE_MAJOR) { j = t % NR; l = t / NR; } else { l = t % L; j = t / L; }
+    bfly_index<LM>(t, NR, L, l, j);
     const int k = j % Ns;
     double2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int n = j + r * NR;
-      v[r] = LINE_MAJOR ? a[l * N + n] : a[n * L + l];
-    }
-    if (Ns > 1) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        double2 w = tw[r * k * tstr];
-        if (sgn > 0) w.y = -w.y;
-        v[r] = cmul(v[r], w);
-      }
-    }
+    for (int r = 0; r < R; ++r) v[r] = src(l, j + r * NR);
+    if (Ns > 1) twiddle<R>(v, k, tstr, sgn, tw);
     dft_small<R>(v, sgn, tw, N);
     const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int n = base + r * Ns;
-      if (LINE_MAJOR) b[l * N + n] = v[r]; else b[n * L + l] = v[r];
-    }
+    for (int r = 0; r < R; ++r) dst(l, base + r * Ns, v[r]);
   }
 }
 
-// Full transform; returns the buffer holding the result.
-template <bool LINE_MAJOR>
-__device__ double2 *stockham(double2 *a, double2 *b, int N, int L, const int *rad, int np,
-                             int sgn, const double2 *tw) {
-  int Ns = 1;
-  for (int p = 0; p < np; ++p) {
-    const int R = rad[p];
-    switch (R) {
-      case 4: stockham_pass<4, LINE_MAJOR>(a, b, N, L, Ns, sgn, tw); break;
-      case 2: stockham_pass<2, LINE_MAJOR>(a, b, N, L, Ns, sgn, tw); break;
-      case 3: stockham_pass<3, LINE_MAJOR>(a, b, N, L, Ns, sgn, tw); break;
-      case 5: stockham_pass<5, LINE_MAJOR>(a, b, N, L, Ns, sgn, tw); break;
-      default: stockham_pass<7, LINE_MAJOR>(a, b, N, L, Ns, sgn, tw); break;
-    }
+template <bool LM, class Src, class Dst>
+__device__ __forceinline__ void run_stream(int R, int N, int L, int Ns, int sgn, const double2 *tw,
+                                           const Src &src, const Dst &dst) {
+  switch (R) {
+    case 16: pass_stream<16, LM>(N, L, Ns, sgn, tw, src, dst); break;
+    case 8: pass_stream<8, LM>(N, L, Ns, sgn, tw, src, dst); break;
+    case 4: pass_stream<4, LM>(N, L, Ns, sgn, tw, src, dst); break;
+    case 2: pass_stream<2, LM>(N, L, Ns, sgn, tw, src, dst); break;
+    case 3: pass_stream<3, LM>(N, L, Ns, sgn, tw, src, dst); break;
+    case 5: pass_stream<5, LM>(N, L, Ns, sgn, tw, src, dst); break;
+    default: pass_stream<7, LM>(N, L, Ns, sgn, tw, src, dst); break;
+  }
+}
+
+template <bool LM>
+struct SmemDst {
+  double2 *a; int N, L;
+  __device__ __forceinline__ void operator()(int l, int n, double2 v) const { a[sidx<LM>(l, n, N, L)] = v; }
+};
+template <bool LM>
+struct SmemSrc {
+  const double2 *a; int N, L;
+  __device__ __forceinline__ double2 operator()(int l, int n) const { return a[sidx<LM>(l, n, N, L)]; }
+};
+
+// Transform of L lines.  The first pass streams from ``src`` into shared
+// buffer a; inner passes ping-pong between a and b; the last pass streams to
+// ``dst`` when LAST_TO_DST, otherwise it lands in shared memory too.  Returns
+// the shared buffer holding the result (meaningful when !LAST_TO_DST).
+template <bool LM, bool LAST_TO_DST, class Src, class Dst>
+__device__ double2 *fft_lines(double2 *a, double2 *b, int N, int L, const int *rad, int np, int sgn,
+                              const double2 *tw, const Src &src, const Dst &dst) {
+  if (np == 1 && LAST_TO_DST) {
+    run_stream<LM>(rad[0], N, L, 1, sgn, tw, src, dst);
+    return a;
+  }
+  run_stream<LM>(rad[0], N, L, 1, sgn, tw, src, SmemDst<LM>{a, N, L});
+  __syncthreads();
+  int Ns = rad[0];
+  const int nin = LAST_TO_DST ? np - 1 : np;
+  for (int p = 1; p < nin; ++p) {
+    run_stream<LM>(rad[p], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, SmemDst<LM>{b, N, L});
     __syncthreads();
     double2 *t = a; a = b; b = t;
-    Ns *= R;
+    Ns *= rad[p];
   }
+  if (LAST_TO_DST) run_stream<LM>(rad[np - 1], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, dst);
   return a;
 }
 
-// Lines per block: row pairs of the y transforms, ky columns of the z
-// transform.  Shared memory per block: two (lines x N) complex buffers plus
-// the N twiddles.
-__host__ __device__ __forceinline__ int fft_y_pairs(int nym) {
-  int p = FFT_ELEMS / nym;
-  if (p > 8) p = 8;
-  if (p < 1) p = 1;
-  return p;
+// Lines per block and shared memory: two (lines x N) buffers when the
+// transform has a pass between two shared-memory stages, otherwise one, plus
+// the N twiddles; lines are capped so that a block stays within ~100 KB.
+__host__ __device__ __forceinline__ int fft_nbuf(int np, bool last_to_dst) {
+  const int smem_stages = last_to_dst ? np - 1 : np;   // passes that write shared memory
+  return smem_stages >= 2 ? 2 : 1;
 }
-__host__ __device__ __forceinline__ int fft_z_lines(int nzm) {
-  int l = FFT_ELEMS / nzm;
-  if (l > 16) l = 16;
-  if (l < 1) l = 1;
-  return l;
+__host__ __device__ __forceinline__ int fft_lines_per_block(int N, int nbuf, int cap) {
+  int l = (100 * 1024) / (16 * N * nbuf);
+  if (l > cap) l = cap;
+  return l < 1 ? 1 : l;
 }
-__host__ __device__ __forceinline__ int fft_smem_bytes(int n, int lines) {
-  return (2 * lines + 1) * n * 16;
+__host__ __device__ __forceinline__ int fft_y_pairs(const BoxDev &B) {
+  return fft_lines_per_block(B.nym, fft_nbuf(B.fft_y_np, false), 16);
+}
+__host__ __device__ __forceinline__ int fft_z_lines(const BoxDev &B) {
+  const int l = fft_lines_per_block(B.nzm, fft_nbuf(B.fft_z_np, true), 16);
+  return l < B.nymh ? l : B.nymh;
+}
+__host__ __device__ __forceinline__ int fft_y_smem(const BoxDev &B) {
+  return (fft_nbuf(B.fft_y_np, false) * fft_y_pairs(B) + 1) * B.nym * 16;
+}
+__host__ __device__ __forceinline__ int fft_z_smem(const BoxDev &B) {
+  return (fft_nbuf(B.fft_z_np, true) * fft_z_lines(B) + 1) * B.nzm * 16;
 }
 
 // ---------------------------------------------------------------------------
-// y forward: rows (k, i) of length nym -> spec[k][i][ky], ky <= nym/2.
-// FROM_VEL: the row values are the divergence of (vx, vy, vz) times 1/(al dt)
-// computed on the fly; otherwise they are read from phi (the dph buffer).
+// y forward: rows (k, i) of length nym -> spec[k][i][ky], ky <= nym/2.  Two
+// real rows form one complex line.  FROM_VEL: the row values are the
+// divergence of (vx, vy, vz) times 1/(al dt) (CalcLocalDivergence.F90:28-38),
+// computed in the first pass; otherwise they are read from phi (dph).
 // ---------------------------------------------------------------------------
+template <bool FROM_VEL>
+struct YSrc {
+  const BoxDev *B;
+  int k, i0;
+  double usdtal, udx3m;
+  __device__ __forceinline__ double row(int i, int j) const {
+    if (i >= B->nzm) return 0.0;
+    const int N = B->nym, nzm = B->nzm;
+    const long long P = B->plane;
+    const long long o = (long long)k * P + (long long)i * N + j;
+    if (!FROM_VEL) return B->phi[o];
+    const int ip = i == nzm - 1 ? 0 : i + 1;
+    const int jp = j == N - 1 ? 0 : j + 1;
+    const double dq = (B->vz[(long long)k * P + (long long)ip * N + j] - B->vz[o]) * B->dz
+                    + (B->vy[(long long)k * P + (long long)i * N + jp] - B->vy[o]) * B->dy
+                    + (B->vx[o + P] - B->vx[o]) * udx3m;
+    return dq * usdtal;
+  }
+  __device__ __forceinline__ double2 operator()(int p, int j) const {
+    const int i = i0 + 2 * p;
+    return make_double2(row(i, j), row(i + 1, j));
+  }
+};
+struct NoDst {
+  __device__ __forceinline__ void operator()(int, int, double2) const {}
+};
+
 template <bool FROM_VEL>
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
   extern __shared__ double2 fsm[];
@@ -173,45 +297,28 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
   const BoxScalars *S = B.sc;
   if (S->status != 0) return;
   const int N = B.nym, nzm = B.nzm;
-  const int Pp = fft_y_pairs(N);
+  const int Pp = fft_y_pairs(B);
   const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / groups;
   const int i0 = (tile - k * groups) * 2 * Pp;
-  double2 *a = fsm, *bb = fsm + Pp * N, *tws = fsm + 2 * Pp * N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = __ldg(B.twy + t);
-  const long long P = B.plane;
-  const double usdtal = FROM_VEL ? 1.0 / (S->dt * S->al) : 0.0;
-  const double udx3m = FROM_VEL ? tabk(B, T_UDX3M, k) : 0.0;
-  for (int t = threadIdx.x; t < 2 * Pp * N; t += blockDim.x) {
-    const int row = t / N, j = t - row * N;
-    const int i = i0 + row;
-    double v = 0.0;
-    if (i < nzm) {
-      const long long o = (long long)k * P + (long long)i * N + j;
-      if (FROM_VEL) {
-        const int ip = i == nzm - 1 ? 0 : i + 1;
-        const int jp = j == N - 1 ? 0 : j + 1;
-        const double dq = (B.vz[(long long)k * P + (long long)ip * N + j] - B.vz[o]) * B.dz
-                        + (B.vy[(long long)k * P + (long long)i * N + jp] - B.vy[o]) * B.dy
-                        + (B.vx[o + P] - B.vx[o]) * udx3m;
-        v = dq * usdtal;
-      } else {
-        v = B.phi[o];
-      }
-    }
-    const int p = row >> 1;
-    if (row & 1) a[p * N + j].y = v; else a[p * N + j].x = v;
-  }
+  const int nb = fft_nbuf(B.fft_y_np, false);
+  double2 *a = fsm, *bb = fsm + (nb - 1) * Pp * N, *tws = fsm + nb * Pp * N;
+  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twy + t);
   __syncthreads();
-  const double2 *r = stockham<true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, tws);
+  YSrc<FROM_VEL> src{&B, k, i0, FROM_VEL ? 1.0 / (S->dt * S->al) : 0.0,
+                     FROM_VEL ? tabk(B, T_UDX3M, k) : 0.0};
+  a = fft_lines<true, false>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, tws, src, NoDst{});
+  __syncthreads();
+  // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
+  // B = (Z_q - conj Z_{N-q}) / (2i)
   const int nh = B.nymh;
-  for (int t = threadIdx.x; t < Pp * nh; t += blockDim.x) {
+  for (int t = threadIdx.x; t < Pp * nh; t += FFT_T) {
     const int p = t / nh, q = t - p * nh;
     const int i = i0 + 2 * p;
     if (i >= nzm) continue;
-    const double2 z = r[p * N + q];
-    const double2 zn = r[p * N + (q == 0 ? 0 : N - q)];
+    const double2 z = a[p * N + q];
+    const double2 zn = a[p * N + (q == 0 ? 0 : N - q)];
     const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
     const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
     const long long base = ((long long)k * nzm + i) * nh + q;
@@ -224,6 +331,23 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
 // z transform in place on spec[k][kz][ky] for a tile of L consecutive ky.
 // Forward transforms divide by nym*nzm (SolvePressureCorrection.F90:105).
 // ---------------------------------------------------------------------------
+struct ZSrc {
+  const double2 *spec; int nh, ky0;
+  __device__ __forceinline__ double2 operator()(int l, int n) const {
+    const int ky = ky0 + l;
+    return ky < nh ? spec[(long long)n * nh + ky] : make_double2(0.0, 0.0);
+  }
+};
+struct ZDst {
+  double2 *spec; int nh, ky0; double norm; bool scale;
+  __device__ __forceinline__ void operator()(int l, int n, double2 v) const {
+    const int ky = ky0 + l;
+    if (ky >= nh) return;
+    if (scale) { v.x = v.x / norm; v.y = v.y / norm; }
+    spec[(long long)n * nh + ky] = v;
+  }
+};
+
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
@@ -231,31 +355,18 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn
   if (!B.active || ns >= B.nsst) return;
   if (B.sc->status != 0) return;
   const int N = B.nzm, nh = B.nymh;
-  const int L = fft_z_lines(N);
+  const int L = fft_z_lines(B);
   const int ntl = (nh + L - 1) / L;
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / ntl;
   const int ky0 = (tile - k * ntl) * L;
-  double2 *a = fsm, *bb = fsm + L * N, *tws = fsm + 2 * L * N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = __ldg(B.twz + t);
-  double2 *spec = B.spec + (long long)k * N * nh;
-  for (int t = threadIdx.x; t < L * N; t += blockDim.x) {
-    const int l = t % L, n = t / L;
-    const int ky = ky0 + l;
-    a[n * L + l] = ky < nh ? spec[(long long)n * nh + ky] : make_double2(0.0, 0.0);
-  }
+  const int nb = fft_nbuf(B.fft_z_np, true);
+  double2 *a = fsm, *bb = fsm + (nb - 1) * L * N, *tws = fsm + nb * L * N;
+  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twz + t);
   __syncthreads();
-  const double2 *r = stockham<false>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, tws);
-  const double norm = (double)(B.nzm * B.nym);
-  for (int t = threadIdx.x; t < L * N; t += blockDim.x) {
-    const int l = t % L, n = t / L;
-    const int ky = ky0 + l;
-    if (ky < nh) {
-      double2 v = r[n * L + l];
-      if (sgn < 0) { v.x = v.x / norm; v.y = v.y / norm; }
-      spec[(long long)n * nh + ky] = v;
-    }
-  }
+  double2 *spec = B.spec + (long long)k * N * nh;
+  fft_lines<false, true>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, tws, ZSrc{spec, nh, ky0},
+                         ZDst{spec, nh, ky0, (double)(B.nzm * B.nym), sgn < 0});
 }
 
 // ---------------------------------------------------------------------------
@@ -330,8 +441,34 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
 // ---------------------------------------------------------------------------
 // y inverse (complex-to-real, unnormalised): spec[k][i][ky] -> phi[k][i][j].
 // As in a c2r transform, the imaginary parts of the ky = 0 and ky = nym/2
-// coefficients are ignored.
+// coefficients are ignored.  Two rows are recovered from one complex line
+// Z = A + i B.
 // ---------------------------------------------------------------------------
+struct YInvSrc {
+  const double2 *spec; int N, nh, nzm, i0; bool even;
+  __device__ __forceinline__ double2 coef(int i, int n) const {
+    if (i >= nzm) return make_double2(0.0, 0.0);
+    const int q = n < nh ? n : N - n;
+    double2 c = spec[(long long)i * nh + q];
+    if (q == 0 || (even && 2 * q == N)) c.y = 0.0;
+    else if (n >= nh) c.y = -c.y;
+    return c;
+  }
+  __device__ __forceinline__ double2 operator()(int p, int n) const {
+    const int i = i0 + 2 * p;
+    const double2 A = coef(i, n), Bv = coef(i + 1, n);
+    return make_double2(A.x - Bv.y, A.y + Bv.x);
+  }
+};
+struct YInvDst {
+  double *phi; int N, nzm, i0;
+  __device__ __forceinline__ void operator()(int p, int j, double2 v) const {
+    const int i = i0 + 2 * p;
+    if (i < nzm) phi[(long long)i * N + j] = v.x;
+    if (i + 1 < nzm) phi[(long long)(i + 1) * N + j] = v.y;
+  }
+};
+
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
@@ -339,41 +476,18 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns) {
   if (!B.active || ns >= B.nsst) return;
   if (B.sc->status != 0) return;
   const int N = B.nym, nzm = B.nzm, nh = B.nymh;
-  const int Pp = fft_y_pairs(N);
+  const int Pp = fft_y_pairs(B);
   const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / groups;
   const int i0 = (tile - k * groups) * 2 * Pp;
-  double2 *a = fsm, *bb = fsm + Pp * N, *tws = fsm + 2 * Pp * N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = __ldg(B.twy + t);
-  const bool even = (N % 2) == 0;
-  for (int t = threadIdx.x; t < Pp * N; t += blockDim.x) {
-    const int p = t / N, n = t - p * N;
-    const int i = i0 + 2 * p;
-    double2 A = make_double2(0.0, 0.0), Bv = make_double2(0.0, 0.0);
-    const int q = n < nh ? n : N - n;
-    const bool conj = n >= nh;
-    const bool realonly = (q == 0) || (even && q == N / 2);
-    if (i < nzm) {
-      A = B.spec[((long long)k * nzm + i) * nh + q];
-      if (realonly) A.y = 0.0; else if (conj) A.y = -A.y;
-    }
-    if (i + 1 < nzm) {
-      Bv = B.spec[((long long)k * nzm + i + 1) * nh + q];
-      if (realonly) Bv.y = 0.0; else if (conj) Bv.y = -Bv.y;
-    }
-    a[p * N + n] = make_double2(A.x - Bv.y, A.y + Bv.x);
-  }
+  const int nb = fft_nbuf(B.fft_y_np, true);
+  double2 *a = fsm, *bb = fsm + (nb - 1) * Pp * N, *tws = fsm + nb * Pp * N;
+  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twy + t);
   __syncthreads();
-  const double2 *r = stockham<true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, +1, tws);
-  const long long P = B.plane;
-  for (int t = threadIdx.x; t < 2 * Pp * N; t += blockDim.x) {
-    const int row = t / N, j = t - row * N;
-    const int i = i0 + row;
-    if (i >= nzm) continue;
-    const double2 z = r[(row >> 1) * N + j];
-    B.phi[(long long)k * P + (long long)i * N + j] = (row & 1) ? z.y : z.x;
-  }
+  fft_lines<true, true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, +1, tws,
+                        YInvSrc{B.spec + (long long)k * nzm * nh, N, nh, nzm, i0, (N % 2) == 0},
+                        YInvDst{B.phi + (long long)k * B.plane, N, nzm, i0});
 }
 
 }  // namespace afid
