@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -65,18 +66,28 @@ struct Batch {
   size_t smem_y = 0, smem_z = 0;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
+  int k1_minb = 2;          // variant of the explicit/forward kernel (tuning)
 };
 
 long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
 
+// FFT plan of length n: radix 16 for every four factors of two, one radix
+// 8, 4 or 2 for the rest, then 3, 5 and 7; passes in increasing radix order
+// so that the large radices run last, in place, with few butterflies.
 int factor_radices(int n, int *rad, int *np) {
-  int m = n, c = 0;
-  while (m % 4 == 0) { rad[c++] = 4; m /= 4; }
-  while (m % 2 == 0) { rad[c++] = 2; m /= 2; }
+  int m = n, a = 0, c = 0;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  int tmp[16];
+  while (a >= 4 && c < 15) { tmp[c++] = 16; a -= 4; }
+  if (a == 3) tmp[c++] = 8; else if (a == 2) tmp[c++] = 4; else if (a == 1) tmp[c++] = 2;
   const int odd[3] = {3, 5, 7};
   for (int q = 0; q < 3; ++q)
-    while (m % odd[q] == 0) { rad[c++] = odd[q]; m /= odd[q]; }
-  if (m != 1 || c > 15) return -1;
+    while (m % odd[q] == 0 && c < 15) { tmp[c++] = odd[q]; m /= odd[q]; }
+  if (m != 1 || c > 15 || c == 0) return -1;
+  // insertion sort, increasing
+  for (int x = 1; x < c; ++x)
+    for (int y = x; y > 0 && tmp[y - 1] > tmp[y]; --y) { int t = tmp[y]; tmp[y] = tmp[y - 1]; tmp[y - 1] = t; }
+  for (int x = 0; x < c; ++x) rad[x] = tmp[x];
   rad[c] = 0;
   *np = c;
   return 0;
@@ -88,8 +99,8 @@ long long tiles_of(const BoxDev &B, int fam) {
     case FAM_COL: return cdiv(B.plane, 256);
     case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
     case FAM_DIAG: return cdiv((long long)B.nxm * B.plane, 1024);
-    case FAM_FY: return (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B.nym));
-    case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B.nzm));
+    case FAM_FY: return (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
+    case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
     case FAM_PX: return cdiv((long long)B.nzm * B.nymh, 256);
   }
   return 0;
@@ -267,8 +278,8 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     BoxDev d = hb->dev;
     d.active = 1;
     devs.push_back(d);
-    const size_t sy = (size_t)fft_smem_bytes(d.nym, fft_y_pairs(d.nym));
-    const size_t sz = (size_t)fft_smem_bytes(d.nzm, fft_z_lines(d.nzm));
+    const size_t sy = (size_t)fft_y_smem(d);
+    const size_t sz = (size_t)fft_z_smem(d);
     if (sy > bt->smem_y) bt->smem_y = sy;
     if (sz > bt->smem_z) bt->smem_z = sz;
   }
@@ -289,6 +300,10 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   }
   CK(cudaMemcpy(bt->d_boxes, devs.data(), sizeof(BoxDev) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(bt->d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+  {
+    const char *e = getenv("AFID_K1_MINB");
+    if (e && atoi(e) == 3) bt->k1_minb = 3;
+  }
   c->batches[key] = bt;
   *out = bt;
   return 0;
@@ -305,7 +320,8 @@ BatchDev bdev(const Batch *bt, int fam) {
 int init_kernel_attrs() {
   static bool done = false;
   if (done) return 0;
-  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
   const int fsm = 200 * 1024;   // lines x N plus twiddles, bounded by the nym, nzm <= 8192 limit
   CK(cudaFuncSetAttribute(k_fft_y_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_y_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
@@ -367,7 +383,10 @@ int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) 
   k_substep_prep<<<nb, 256, 0, s>>>(bt->d_boxes, nb, ns);
   CKL();
   PMARK(pf, AFID_K_PREP);
-  k_explicit_implicit_fwd<<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
+  if (bt->k1_minb == 2)
+    k_explicit_implicit_fwd<2><<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
+  else
+    k_explicit_implicit_fwd<3><<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
   CKL();
   PMARK(pf, AFID_K_EXPLICIT_FWD);
   k_implicit_bwd<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
@@ -1174,8 +1193,8 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   const BoxDev *dbox = (const BoxDev *)(base + o_box);
   const int *doff = (const int *)(base + o_off);
   BatchDev fy{dbox, doff + 0, 1}, fz{dbox, doff + 2, 1}, px{dbox, doff + 4, 1};
-  const size_t sy = (size_t)fft_smem_bytes(nym, fft_y_pairs(nym));
-  const size_t sz = (size_t)fft_smem_bytes(nzm, fft_z_lines(nzm));
+  const size_t sy = (size_t)fft_y_smem(d);
+  const size_t sz = (size_t)fft_z_smem(d);
   k_fft_y_fwd<false><<<off[0][1], FFT_T, sy, st>>>(fy, 0);
   CKL();
   k_fft_z<<<off[1][1], FFT_T, sz, st>>>(fz, 0, -1);

@@ -245,20 +245,36 @@ constexpr int K1_NT = K1_TJ * K1_TI;            // threads per block (256)
 constexpr int K1_NSLOT = 4;
 constexpr int K1_NTAB = 14;                     // per-k scalars staged per plane
 constexpr int K1_RING = K1_NSLOT * F_NF * K1_PL;        // doubles
-constexpr int K1_HIST = 2 * 4 * K1_NT;                  // doubles
-constexpr int K1_TABR = 2 * 16;                         // doubles
-constexpr int K1_SMEM = (K1_RING + K1_HIST + K1_TABR) * 8;
+constexpr int K1_TABR = K1_NSLOT * 16;                  // doubles
+constexpr int K1_SMEM = (K1_RING + K1_TABR) * 8;
 
 // per-k scalar slots staged in shared memory
 enum K1Tab { KT_UDX3M = 0, KT_UDX3C, KT_AM3SK, KT_AC3SK, KT_AP3SK, KT_AM3CK, KT_AC3CK, KT_AP3CK,
              KT_XSC, KT_XF, KT_YSC, KT_YF, KT_TSC, KT_TF };
 
+// Values of plane k-1 that the stencils at plane k read, kept in registers
+// by the thread of the column (its own column, plus vy at j+1 and vz at i+1).
+struct K1Prev {
+  double vx, vy, vy_jp, vz, vz_ip, t, pr;
+};
+
+// Accessor over the ring (planes k and k+1, 1-cell halo) and the stash of
+// plane k-1.  Every plane-(k-1) access of the stencil formulas is one of the
+// seven stashed values.
 struct RingAcc {
   const double *ring;   // [slot][field][K1_PL]
-  int s_m, s_c, s_p;    // slots of k-1, k, k+1
+  int s_c, s_p;         // slots of k and k+1
   int off;              // (ti+1)*K1_HJ + tj+1
+  K1Prev prev;
   __device__ __forceinline__ double operator()(int f, int dk, int dj, int di) const {
-    const int s = dk < 0 ? s_m : (dk > 0 ? s_p : s_c);
+    if (dk < 0) {
+      if (f == F_VX) return prev.vx;
+      if (f == F_VY) return dj > 0 ? prev.vy_jp : prev.vy;
+      if (f == F_VZ) return di > 0 ? prev.vz_ip : prev.vz;
+      if (f == F_T) return prev.t;
+      return prev.pr;
+    }
+    const int s = dk > 0 ? s_p : s_c;
     return ring[(s * F_NF + f) * K1_PL + off + di * K1_HJ + dj];
   }
 };
@@ -269,6 +285,7 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int k) {
   switch (t) {
@@ -291,21 +308,23 @@ __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int 
 
 // ---------------------------------------------------------------------------
 // K1: explicit terms + implicit rhs + forward elimination for all four
-// fields, one thread per (j, i) column marching k upwards.  Shared memory
-// holds (a) a ring of four x-planes of vx, vy, vz, temp, pr (tile plus a
-// 1-cell halo), fetched two planes ahead, (b) the RK history of the next
-// plane and (c) the per-k metric and LU scalars of the next plane; all three
-// arrive through cp.async while the current plane is computed, so a plane
-// costs one barrier and no exposed load latency.  Writes the RK history
-// (rux.. = H) and the forward-sweep values y of each solve; the temperature
-// sweep starts from y(1) = 0 and the missing contribution of its wall row is
-// added by K2 (the solve is linear in y(1)).
+// fields, one thread per (j, i) column marching k upwards.  MINB is the
+// occupancy target (resident blocks per SM; 3 caps registers at 80, 2 at
+// 128).  Shared memory holds a ring of four x-planes of vx, vy, vz, temp, pr (tile plus a 1-cell
+// halo) and of the per-k metric and LU scalars; plane k+3 is fetched with
+// cp.async while plane k is computed, so each load has two planes of compute
+// to arrive in.  Plane k-1 is not read from the ring: the seven values of it
+// that the stencils need are kept in registers.  The RK history of plane k+2
+// is loaded into registers two planes ahead.  Writes the RK history (rux.. =
+// H) and the forward-sweep values y of each solve; the temperature sweep
+// starts from y(1) = 0 and the missing contribution of its wall row is added
+// by K2 (the solve is linear in y(1)).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt, int ns) {
+template <int MINB>
+__global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev bt, int ns) {
   extern __shared__ double k1sm[];
   double *ring = k1sm;
-  double *hring = k1sm + K1_RING;            // [2][4][K1_NT]
-  double *tring = hring + K1_HIST;           // [2][16]
+  double *tring = k1sm + K1_RING;            // [slot][16]
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
@@ -332,7 +351,6 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
   const double dz_ = B.dz;
 
   const double *fld[F_NF] = {B.vx, B.vy, B.vz, B.temp, B.pr};
-  double *hist[4] = {B.rux, B.ruy, B.ruz, B.rutemp};
 
   // this thread's halo elements (r0 = tid always < K1_PL; r1 = tid + K1_NT if < K1_PL)
   const int r1 = tid + K1_NT;
@@ -348,7 +366,7 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
       g1 = (long long)ii * nym + jj;
     }
   }
-  auto load_plane = [&](int p) {
+  auto load_plane = [&](int p) {      // plane p and its per-k scalars into slot p & 3
     double *dst = ring + (p & (K1_NSLOT - 1)) * F_NF * K1_PL;
     const long long po = (long long)p * P;
 #pragma unroll
@@ -356,41 +374,43 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
       cp_async8(dst + f * K1_PL + tid, fld[f] + po + g0);
       if (has1) cp_async8(dst + f * K1_PL + r1, fld[f] + po + g1);
     }
+    if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + (p & (K1_NSLOT - 1)) * 16 + tid, k1_tab_src(B, tid, p));
   };
-  auto load_next = [&](int k) {          // history and scalars of plane k
-    double *hd = hring + (k & 1) * 4 * K1_NT;
-    if (inside) {
-      const long long o = (long long)k * P + col;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) cp_async8(hd + q * K1_NT + tid, hist[q] + o);
+  // RK history of a plane, straight into registers
+  auto load_hist = [&](int p, double (&h)[4]) {
+    if (inside && p <= nxm - 1) {
+      const long long o = (long long)p * P + col;
+      h[0] = B.rux[o]; h[1] = B.ruy[o]; h[2] = B.ruz[o]; h[3] = B.rutemp[o];
     }
-    if (tid < K1_NTAB) cp_async8(tring + (k & 1) * 16 + tid, k1_tab_src(B, tid, k));
   };
 
   RingAcc acc;
   acc.ring = ring;
   acc.off = (ti + 1) * K1_HJ + tj + 1;
+  acc.prev = K1Prev{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
   // forward-sweep carries
   double yX = inside ? B.wall[col] : 0.0;   // rhs(1,j,i) left by the last vz solve
   double yY = 0.0, yZ = 0.0, yT = 0.0;
+  double h0[4] = {0.0, 0.0, 0.0, 0.0}, h1[4] = {0.0, 0.0, 0.0, 0.0}, h2[4] = {0.0, 0.0, 0.0, 0.0};
 
   load_plane(0);
   load_plane(1);
-  load_next(0);
   cp_async_commit();
-  cp_async_wait_all();
+  if (2 <= nx - 1) load_plane(2);
+  cp_async_commit();
+  load_hist(0, h0);
+  load_hist(1, h1);
+  cp_async_wait_1();
   __syncthreads();
 
   for (int kc = 0; kc < nxm; ++kc) {
-    if (kc + 2 <= nx - 1) load_plane(kc + 2);
-    if (kc + 1 <= nxm - 1) load_next(kc + 1);
+    if (kc + 3 <= nx - 1) load_plane(kc + 3);
     cp_async_commit();
+    load_hist(kc + 2, h2);
     acc.s_c = kc & 3;
-    acc.s_m = (kc + 3) & 3;   // kc-1 (unused at kc = 0 except through dkm = 0)
     acc.s_p = (kc + 1) & 3;
-    const double *tk = tring + (kc & 1) * 16;
-    const double *hk = hring + (kc & 1) * 4 * K1_NT;
+    const double *tk = tring + (kc & 3) * 16;
     if (inside) {
       const long long o = (long long)kc * P + col;
       const int dkm = kc == 0 ? 0 : -1;
@@ -401,7 +421,7 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
       {
         const double H = h_vy(acc, c, udx3m_k, dkm, dkp);
         const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
-        const double r = rhs_vyz(H, hk[1 * K1_NT + tid], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
+        const double r = rhs_vyz(H, h0[1], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
                                  acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
         B.ruy[o] = H;
         const double bb = r * tk[KT_YSC];
@@ -411,7 +431,7 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
       {
         const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
         const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
-        const double r = rhs_vyz(H, hk[2 * K1_NT + tid], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
+        const double r = rhs_vyz(H, h0[2], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
                                  acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
         B.ruz[o] = H;
         const double bb = r * tk[KT_YSC];
@@ -423,7 +443,7 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
         const double am_c = tk[KT_AM3CK], ac_c = tk[KT_AC3CK], ap_c = tk[KT_AP3CK];
         {
           const double H = h_vx(acc, c, udx3c_k);
-          const double r = rhs_vx(H, hk[0 * K1_NT + tid], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
+          const double r = rhs_vx(H, h0[0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
                                   acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
                                   am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
           B.rux[o] = H;
@@ -433,7 +453,7 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
         }
         {
           const double H = h_temp(acc, c, udx3c_k);
-          const double r = rhs_temp(H, hk[3 * K1_NT + tid], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
+          const double r = rhs_temp(H, h0[3], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
                                     acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
           B.rutemp[o] = H;
           const double bb = r * tk[KT_TSC];
@@ -441,10 +461,21 @@ __global__ void __launch_bounds__(K1_NT, 3) k_explicit_implicit_fwd(BatchDev bt,
           B.ybuf[3][o] = yT;
         }
       }
+      // stash what plane kc+1 will need of this plane
+      acc.prev.vx = acc(F_VX, 0, 0, 0);
+      acc.prev.vy = acc(F_VY, 0, 0, 0);
+      acc.prev.vy_jp = acc(F_VY, 0, 1, 0);
+      acc.prev.vz = acc(F_VZ, 0, 0, 0);
+      acc.prev.vz_ip = acc(F_VZ, 0, 0, 1);
+      acc.prev.t = acc(F_T, 0, 0, 0);
+      acc.prev.pr = acc(F_PR, 0, 0, 0);
     }
-    cp_async_wait_all();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { h0[q] = h1[q]; h1[q] = h2[q]; }
+    cp_async_wait_1();
     __syncthreads();
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
