@@ -33,7 +33,7 @@ EXPORTS = [
     "afid_solve_pressure_correction", "afid_correct_velocity", "afid_correct_pressure",
     "afid_calc_max_cfl", "afid_check_divergence", "afid_calc_plate_nu", "afid_step",
     "afid_step_graph", "afid_substep", "afid_step_profiled",
-    "afid_solve_pressure_correction_noalloc",
+    "afid_solve_pressure_correction_noalloc", "afid_box_set_tuning",
 ]
 
 KERNELS = ["diag", "finalize", "prep", "explicit_fwd", "implicit_bwd", "fft_y_fwd", "fft_z_fwd",
@@ -107,6 +107,7 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_substep": ([vp, ip, i, i], i),
         "afid_step_profiled": ([vp, ip, i, i, dp, ip, i], i),
         "afid_solve_pressure_correction_noalloc": ([vp, i, i, i, dp, d, d, d, vp], i),
+        "afid_box_set_tuning": ([vp, i, i, i, i], i),
     }
     for name in ("explicit_terms_vx", "explicit_terms_vy", "explicit_terms_vz",
                  "explicit_terms_temp", "implicit_and_update_vx", "implicit_and_update_vy",

@@ -301,8 +301,11 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   CK(cudaMemcpy(bt->d_boxes, devs.data(), sizeof(BoxDev) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(bt->d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
   {
+    long long w2 = 0, w3 = 0;
+    for (const BoxDev &d : devs) (d.k1_minb == 3 ? w3 : w2) += d.fsize;
+    bt->k1_minb = w3 > w2 ? 3 : 2;
     const char *e = getenv("AFID_K1_MINB");
-    if (e && atoi(e) == 3) bt->k1_minb = 3;
+    if (e && (atoi(e) == 2 || atoi(e) == 3)) bt->k1_minb = atoi(e);
   }
   c->batches[key] = bt;
   *out = bt;
@@ -606,6 +609,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   d.pec = std::sqrt(p->pra * p->ray);
   d.tempbp = p->tempbp; d.temptp = p->temptp;
   d.hist_cap = HIST_CAP;
+  d.k1_minb = 2;
   const size_t fb = 9 * (size_t)s.fsize * sizeof(double);
   const size_t sb = (size_t)s.scratch * sizeof(double);
   const size_t mb = (size_t)s.small * sizeof(double);
@@ -800,6 +804,33 @@ int afid_box_history(afid_ctx *c, int id, afid_step_record *out, int max_records
     out[r].nu_bot = src[4]; out[r].nu_top = src[5]; out[r].vmax_y = src[6]; out[r].vmax_z = src[7];
   }
   return n;
+}
+
+int afid_box_set_tuning(afid_ctx *c, int id, int fft_y_lines, int fft_z_lines, int k1_minb) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  BoxDev &d = hb->dev;
+  if (fft_y_lines < 0 || fft_y_lines > fft_max_lines(d.nym, fft_nbuf(d.fft_y_np, false)))
+    return fail(AFID_EINVAL, "fft_y_lines %d out of range", fft_y_lines);
+  if (fft_z_lines < 0 || fft_z_lines > fft_max_lines(d.nzm, fft_nbuf(d.fft_z_np, true)))
+    return fail(AFID_EINVAL, "fft_z_lines %d out of range", fft_z_lines);
+  if (k1_minb != 0 && k1_minb != 2 && k1_minb != 3) return fail(AFID_EINVAL, "k1_minb must be 0, 2 or 3");
+  rc = set_device(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  d.fy_lines = fft_y_lines;
+  d.fz_lines = fft_z_lines;
+  d.k1_minb = k1_minb ? k1_minb : 2;
+  // batches hold copies of the descriptor and tile tables: drop them
+  for (auto it = c->batches.begin(); it != c->batches.end();) {
+    bool has = false;
+    for (int x : it->first) has |= (x == id);
+    if (has) { free_batch(it->second); it = c->batches.erase(it); }
+    else ++it;
+  }
+  return sync_self(hb);
 }
 
 // ---- routine-level entry points -------------------------------------------

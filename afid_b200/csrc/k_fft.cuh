@@ -242,11 +242,16 @@ __host__ __device__ __forceinline__ int fft_lines_per_block(int N, int nbuf, int
   return l < 1 ? 1 : l;
 }
 __host__ __device__ __forceinline__ int fft_y_pairs(const BoxDev &B) {
+  if (B.fy_lines > 0) return B.fy_lines;
   return fft_lines_per_block(B.nym, fft_nbuf(B.fft_y_np, false), 16);
 }
 __host__ __device__ __forceinline__ int fft_z_lines(const BoxDev &B) {
-  const int l = fft_lines_per_block(B.nzm, fft_nbuf(B.fft_z_np, true), 16);
+  const int l = B.fz_lines > 0 ? B.fz_lines : fft_lines_per_block(B.nzm, fft_nbuf(B.fft_z_np, true), 16);
   return l < B.nymh ? l : B.nymh;
+}
+// largest admissible tuning values (shared memory of one block <= 200 KB)
+__host__ __device__ __forceinline__ int fft_max_lines(int N, int nbuf) {
+  return (200 * 1024) / (16 * N * nbuf) - 1;
 }
 __host__ __device__ __forceinline__ int fft_y_smem(const BoxDev &B) {
   return (fft_nbuf(B.fft_y_np, false) * fft_y_pairs(B) + 1) * B.nym * 16;

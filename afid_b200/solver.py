@@ -160,6 +160,11 @@ class Box:
         _lib.check(self._L.afid_box_download(self.ctx.h, self.id, _lib.FIELDS[field], _lib.dptr(buf)))
         return np.ascontiguousarray(buf.transpose(2, 1, 0))
 
+    def set_tuning(self, fft_y_lines: int = 0, fft_z_lines: int = 0, k1_minb: int = 0):
+        """Launch shapes of this box's kernels (results do not depend on them)."""
+        _lib.check(self._L.afid_box_set_tuning(self.ctx.h, self.id, fft_y_lines, fft_z_lines, k1_minb))
+        self.tuning = (fft_y_lines, fft_z_lines, k1_minb)
+
     def reset(self, dt: float = 0.0):
         _lib.check(self._L.afid_box_reset(self.ctx.h, self.id, dt))
 

@@ -39,9 +39,15 @@ sys.path.insert(0, ROOT)
 METRIC = "Mpoint-steps/s FP64 (RK3 step, cells = nxm*nym*nzm)"
 UNIT = "Mpoint-steps/s"
 
-# DRAM traffic per cell of each kernel from an ncu capture (bytes read +
-# written / (nxm*nym*nzm)); see profiles/ for the capture and its command.
-NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {}
+# DRAM traffic per cell of each kernel, dram__bytes_read.sum +
+# dram__bytes_write.sum / (nxm*nym*nzm), from the ncu --set full capture of
+# the 193x384x384 box summarised in profiles/ncu_full_substep_193x384x384.md
+# (traffic scales with the number of cells; the kernels have the same
+# per-cell structure at every size).
+NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
+    "explicit_fwd": 135.8, "implicit_bwd": 94.5, "fft_y_fwd": 31.8, "fft_z_fwd": 14.3,
+    "poisson_x": 34.0, "fft_z_inv": 14.3, "fft_y_inv": 14.6,
+}
 
 
 # ----------------------------------------------------------------------------
@@ -66,27 +72,11 @@ def workload_boxes(name: str, rank: int = 0):
                       istr3=7, idtv=0, resid=0.0)], {"workload": "box 193x384x384 Ra=1e9 Pr=1 dt=1e-4",
                                                      "nx": 193, "ny": 384, "nz": 384}
     if name == "batch":
-        return ensemble_boxes(64, seed=1000 + rank), {"workload": "ensemble of 64 boxes, nx in {33,65,97}, "
-                                                      "ny=nz in {32..128}, Ra log-uniform [1e5,1e8]",
-                                                      "boxes": 64}
+        from afid_b200.ensemble import ensemble_configs
+        return ensemble_configs(64, seed=1000 + rank), {
+            "workload": "ensemble of 64 boxes, nx in {33,65,97}, ny=nz in {32..128}, "
+                        "Ra log-uniform [1e5,1e8], Pr in {0.7,1,4.38}", "boxes": 64}
     raise SystemExit(f"unknown workload {name}")
-
-
-def ensemble_boxes(n: int, seed: int):
-    """Per-box sizes and physics drawn from PCG64(seed) (batched ensemble)."""
-    from afid_b200 import BouIn
-    rng = np.random.Generator(np.random.PCG64(seed))
-    out = []
-    for _ in range(n):
-        nxm = int(rng.choice([32, 64, 96]))
-        nyz = int(rng.choice([32, 48, 64, 96, 128]))
-        asp = min(max(nyz / nxm, 1.0), 2.0)
-        ra = float(10 ** rng.uniform(5, 8))
-        pr = float(rng.choice([0.7, 1.0, 4.38]))
-        dt = 2e-4 if ra < 1e7 else 1e-4
-        out.append(BouIn(nxm=nxm, nym=nyz, nzm=nyz, ylen=asp, zlen=asp, ray=ra, pra=pr, dt=dt,
-                         istr3=7, idtv=0, resid=0.0))
-    return out
 
 
 def cells(cfg) -> int:
@@ -278,6 +268,14 @@ def gpu_arm(args):
         boxes.append(b)
     ncell = sum(cells(c) for c in cfgs)
 
+    # launch shapes from the autotuner (cached per GPU and size class)
+    from afid_b200 import autotune
+    tuned = {}
+    if not args.no_tune:
+        tuned = autotune.tune(ctx, cfgs)
+        for b in boxes:
+            autotune.apply(b, tuned)
+
     # warm-up (also captures the CUDA graph of one step)
     ctx.step(boxes, max(args.warmup, 1), graph=True)
     ctx.synchronize()
@@ -377,6 +375,18 @@ def gpu_arm(args):
                "what": "afid_box_upload of the initial fields from pinned host memory, K x "
                        "(afid_step_graph + afid_box_get_scalars), afid_box_download of the final fields"}
 
+    # ---- batched against the plain one-box-at-a-time loop (ensemble workload)
+    batched = None
+    if args.workload == "batch":
+        from afid_b200.ensemble import run_plain, reset_boxes
+        reset_boxes(boxes, seed0=rank * 1000)
+        t_plain = run_plain(ctx, boxes, args.steps, graph=True)
+        batched = {"plain_value": world * ncell * args.steps / t_plain / 1e6,
+                   "plain_ms_per_step": t_plain * 1e3 / args.steps,
+                   "speedup_vs_plain": (world * ncell * args.steps / t_plain / 1e6) and value / (
+                       world * ncell * args.steps / t_plain / 1e6),
+                   "plain": "the same boxes and steps, one box at a time, a CUDA graph per box step"}
+
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -398,11 +408,52 @@ def gpu_arm(args):
             "gpu_launches": int(round(launches_per_step * args.steps)), "clocks": clk,
             "status": statuses,
         }
+        if batched is not None:
+            line["batched"] = batched
+        if tuned:
+            line["tuning"] = {k: {q: v[q] for q in ("fft_y_lines", "fft_z_lines", "k1_minb")}
+                              for k, v in tuned.items()}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def serve_arm(args):
+    """Served stream: Poisson arrivals at each rate, continuous batching
+    against the plain one-request-at-a-time loop."""
+    import torch
+
+    from afid_b200 import Context
+    from afid_b200.serve import request_stream, serve, serve_mix, serve_plain
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    free, total = torch.cuda.mem_get_info(local)
+    budget = int(free * 0.8)
+    out = {}
+    for rate in args.rates:
+        reqs = request_stream(args.requests, rate, seed=2000 + rank, steps=args.serve_steps, mix=serve_mix)
+        res_b = serve(ctx, reqs, hbm_budget=budget, quantum=32)
+        reqs = request_stream(args.requests, rate, seed=2000 + rank, steps=args.serve_steps, mix=serve_mix)
+        res_p = serve_plain(ctx, reqs)
+        out[str(rate)] = {"served": res_b, "plain": res_p,
+                          "speedup_vs_plain": res_b["mpoint_steps_s"] / res_p["mpoint_steps_s"]}
+    ctx.close()
+    if rank == 0:
+        best = max(out.values(), key=lambda d: d["served"]["mpoint_steps_s"])
+        line = {"metric": METRIC + "; served stream", "value": best["served"]["mpoint_steps_s"],
+                "unit": UNIT, "n_gpus": world, "steps": args.serve_steps, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Poisson arrivals)",
+                "config": {"workload": f"served stream, {args.requests} requests per rate, "
+                                       f"{args.serve_steps} CFL-adaptive steps each, 90% ensemble sizes + "
+                                       "10% 193x384x384, Ra log-uniform [1e5,1e9]",
+                           "hbm_budget_bytes": budget},
+                "rates": out}
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -414,9 +465,16 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "s384", "batch"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
+    ap.add_argument("--serve", action="store_true", help="run the served-stream benchmark")
+    ap.add_argument("--rates", type=float, nargs="+", default=[10.0, 100.0])
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--serve-steps", type=int, default=200)
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.serve:
+        return serve_arm(args)
     return gpu_arm(args)
 
 

@@ -121,6 +121,11 @@ int afid_box_download(afid_ctx *ctx, int box_id, int field, double *host);
  * status; set dt (values <= 0 keep the current dt). */
 int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
 int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
+/* Launch-shape tuning of one box (no counterpart in the reference):
+ * row pairs per y-FFT block, ky columns per z-FFT block (0 = built-in
+ * choice) and the resident-block target of the explicit/forward kernel
+ * (2 or 3; 0 = 2).  Results do not depend on these values. */
+int afid_box_set_tuning(afid_ctx *ctx, int box_id, int fft_y_lines, int fft_z_lines, int k1_minb);
 /* Copies up to max_records of the most recent per-step records, oldest
  * first; returns the number copied (>= 0) or an error code. */
 int afid_box_history(afid_ctx *ctx, int box_id, afid_step_record *out, int max_records);

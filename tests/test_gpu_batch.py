@@ -92,3 +92,20 @@ def test_fft_size_rule(ctx):
     from afid_b200._lib import AfidError
     with pytest.raises((AfidError, ValueError)):
         ctx.add_box(cfg_of(16, 22, 16))
+
+
+def test_launch_shapes_do_not_change_results(ctx):
+    """Tuned launch shapes (FFT lines per block, explicit-kernel occupancy
+    variant) give bit-identical fields."""
+    a = _add(ctx, MIX[2], 21)
+    b = _add(ctx, MIX[2], 21)
+    b.set_tuning(fft_y_lines=1, fft_z_lines=3, k1_minb=3)
+    ctx.step([a], 3)
+    ctx.step([b], 3)
+    for f in FIELDS:
+        assert np.array_equal(a.download(f), b.download(f)), f
+    from afid_b200._lib import AfidError
+    with pytest.raises(AfidError):
+        b.set_tuning(fft_y_lines=10 ** 6)
+    for x in (a, b):
+        ctx.remove_box(x)
