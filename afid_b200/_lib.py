@@ -37,7 +37,7 @@ EXPORTS = [
 ]
 
 KERNELS = ["diag", "finalize", "prep", "explicit_fwd", "implicit_bwd", "fft_y_fwd", "fft_z_fwd",
-           "poisson_x", "fft_z_inv", "fft_y_inv", "correct", "plate_nu"]
+           "poisson_x", "fft_z_inv", "fft_y_inv", "correct", "plate_nu", "divergence"]
 
 
 class BoxParams(C.Structure):

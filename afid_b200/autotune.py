@@ -6,8 +6,9 @@ kernel (afid_step_profiled), and keeps the fastest:
 
 * row pairs per y-FFT block (forward and inverse y transforms),
 * ky columns per z-FFT block (forward and inverse z transforms),
-* the resident-block target of the explicit/forward kernel (2 blocks with
-  up to 128 registers per thread, or 3 with up to 80).
+* the variant of the explicit/forward kernel: 2 resident blocks with up to
+  128 registers per thread, 3 with up to 80, or 2 blocks that compute two
+  x-planes per barrier.
 
 Results do not depend on the shapes (tests/test_gpu_batch.py checks batched
 against single-box results bit for bit), so tuning is purely a speed choice.
@@ -45,7 +46,7 @@ def fft_plan(n: int) -> list[int]:
 
 def _nbuf(np_: int, last_to_dst: bool) -> int:
     stages = np_ - 1 if last_to_dst else np_
-    return 2 if stages >= 2 else 1
+    return 2 if stages >= 1 else 1
 
 
 def _max_lines(n: int, nbuf: int) -> int:
@@ -56,7 +57,7 @@ def candidates(cfg: BouIn) -> dict:
     ny = [v for v in (1, 2, 4, 8, 16) if v <= _max_lines(cfg.nym, _nbuf(len(fft_plan(cfg.nym)), False))]
     nz_max = min(_max_lines(cfg.nzm, _nbuf(len(fft_plan(cfg.nzm)), True)), cfg.nym // 2 + 1)
     nz = [v for v in (1, 2, 4, 8, 16, 32) if v <= nz_max]
-    return {"fft_y_lines": ny or [1], "fft_z_lines": nz or [1], "k1_minb": [2, 3]}
+    return {"fft_y_lines": ny or [1], "fft_z_lines": nz or [1], "k1_minb": [2, 3, 4]}
 
 
 def class_key(cfg: BouIn) -> str:

@@ -66,7 +66,7 @@ struct Batch {
   size_t smem_y = 0, smem_z = 0;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
-  int k1_minb = 2;          // variant of the explicit/forward kernel (tuning)
+  int k1_minb = 2;          // variant of the explicit/forward kernel (tuning, 2..4)
 };
 
 long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
@@ -301,11 +301,13 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   CK(cudaMemcpy(bt->d_boxes, devs.data(), sizeof(BoxDev) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(bt->d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
   {
-    long long w2 = 0, w3 = 0;
-    for (const BoxDev &d : devs) (d.k1_minb == 3 ? w3 : w2) += d.fsize;
-    bt->k1_minb = w3 > w2 ? 3 : 2;
-    const char *e = getenv("AFID_K1_MINB");
-    if (e && (atoi(e) == 2 || atoi(e) == 3)) bt->k1_minb = atoi(e);
+    long long w[5] = {0, 0, 0, 0, 0};
+    for (const BoxDev &d : devs) w[d.k1_minb >= 2 && d.k1_minb <= 4 ? d.k1_minb : 2] += d.fsize;
+    bt->k1_minb = 2;
+    for (int v = 3; v <= 4; ++v)
+      if (w[v] > w[bt->k1_minb]) bt->k1_minb = v;
+    const char *e = getenv("AFID_K1_VARIANT");
+    if (e && atoi(e) >= 2 && atoi(e) <= 4) bt->k1_minb = atoi(e);
   }
   c->batches[key] = bt;
   *out = bt;
@@ -323,11 +325,11 @@ BatchDev bdev(const Batch *bt, int fam) {
 int init_kernel_attrs() {
   static bool done = false;
   if (done) return 0;
-  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
-  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1_SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<2>::SMEM));
   const int fsm = 200 * 1024;   // lines x N plus twiddles, bounded by the nym, nzm <= 8192 limit
-  CK(cudaFuncSetAttribute(k_fft_y_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  CK(cudaFuncSetAttribute(k_fft_y_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fft_y_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   done = true;
@@ -360,10 +362,12 @@ struct Prof {
   } while (0)
 
 int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof *pf = nullptr) {
-  if (from_vel)
-    k_fft_y_fwd<true><<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
-  else
-    k_fft_y_fwd<false><<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
+  if (from_vel) {
+    k_divergence<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
+    CKL();
+    PMARK(pf, AFID_K_DIVERGENCE);
+  }
+  k_fft_y_fwd<<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
   CKL();
   PMARK(pf, AFID_K_FFT_Y_FWD);
   k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, -1);
@@ -386,10 +390,14 @@ int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) 
   k_substep_prep<<<nb, 256, 0, s>>>(bt->d_boxes, nb, ns);
   CKL();
   PMARK(pf, AFID_K_PREP);
-  if (bt->k1_minb == 2)
-    k_explicit_implicit_fwd<2><<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
+  // variants: 2 = two resident blocks, one plane per barrier; 3 = three
+  // resident blocks; 4 = two resident blocks, two planes per barrier
+  if (bt->k1_minb == 3)
+    k_explicit_implicit_fwd<3, 1><<<bt->total[FAM_K1], 256, K1Ring<1>::SMEM, s>>>(bdev(bt, FAM_K1), ns);
+  else if (bt->k1_minb == 4)
+    k_explicit_implicit_fwd<2, 2><<<bt->total[FAM_K1], 256, K1Ring<2>::SMEM, s>>>(bdev(bt, FAM_K1), ns);
   else
-    k_explicit_implicit_fwd<3><<<bt->total[FAM_K1], 256, K1_SMEM, s>>>(bdev(bt, FAM_K1), ns);
+    k_explicit_implicit_fwd<2, 1><<<bt->total[FAM_K1], 256, K1Ring<1>::SMEM, s>>>(bdev(bt, FAM_K1), ns);
   CKL();
   PMARK(pf, AFID_K_EXPLICIT_FWD);
   k_implicit_bwd<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
@@ -816,7 +824,7 @@ int afid_box_set_tuning(afid_ctx *c, int id, int fft_y_lines, int fft_z_lines, i
     return fail(AFID_EINVAL, "fft_y_lines %d out of range", fft_y_lines);
   if (fft_z_lines < 0 || fft_z_lines > fft_max_lines(d.nzm, fft_nbuf(d.fft_z_np, true)))
     return fail(AFID_EINVAL, "fft_z_lines %d out of range", fft_z_lines);
-  if (k1_minb != 0 && k1_minb != 2 && k1_minb != 3) return fail(AFID_EINVAL, "k1_minb must be 0, 2 or 3");
+  if (k1_minb != 0 && (k1_minb < 2 || k1_minb > 4)) return fail(AFID_EINVAL, "k1 variant must be 0, 2, 3 or 4");
   rc = set_device(c);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
@@ -893,7 +901,7 @@ int afid_calc_local_divergence(afid_ctx *c, int id) {
   Batch *bt;
   rc = single_batch(c, id, &bt);
   if (rc) return rc;
-  k_divergence<<<bt->total[FAM_CELL], 256, 0, c->stream>>>(bdev(bt, FAM_CELL));
+  k_divergence<<<bt->total[FAM_COL], 256, 0, c->stream>>>(bdev(bt, FAM_COL), 0);
   CKL();
   return 0;
 }
@@ -1226,7 +1234,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   BatchDev fy{dbox, doff + 0, 1}, fz{dbox, doff + 2, 1}, px{dbox, doff + 4, 1};
   const size_t sy = (size_t)fft_y_smem(d);
   const size_t sz = (size_t)fft_z_smem(d);
-  k_fft_y_fwd<false><<<off[0][1], FFT_T, sy, st>>>(fy, 0);
+  k_fft_y_fwd<<<off[0][1], FFT_T, sy, st>>>(fy, 0);
   CKL();
   k_fft_z<<<off[1][1], FFT_T, sz, st>>>(fz, 0, -1);
   CKL();

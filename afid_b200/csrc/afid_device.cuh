@@ -92,7 +92,7 @@ struct BoxDev {
   int fft_z_radix[16];  // radices of nzm
   int fft_y_np, fft_z_np;
   int active;           // 0 = skipped by every kernel
-  int k1_minb;          // tuning: resident-block target of the explicit/forward kernel (2 or 3)
+  int k1_minb;          // tuning: variant of the explicit/forward kernel (2, 3 or 4)
   int fy_lines;         // tuning: row pairs per y-FFT block (0 = default)
   int fz_lines;         // tuning: ky columns per z-FFT block (0 = default)
   int pad2_;

@@ -1,6 +1,5 @@
 // Pressure Poisson solve of SolvePressureCorrection.F90:35-151 on one GPU:
-//   y: real-to-complex FFT (two real rows packed in one complex line), fused
-//      with the divergence of CalcLocalDivergence.F90 on its load;
+//   y: real-to-complex FFT (two real rows packed in one complex line) of dph;
 //   z: complex FFT along kz on tiles of consecutive ky (in place);
 //   x: one complex tridiagonal per (ky, kz), Thomas in dgttrf/dgttrs order;
 //   then the inverse z and y transforms, the latter writing dph.
@@ -229,12 +228,46 @@ __device__ double2 *fft_lines(double2 *a, double2 *b, int N, int L, const int *r
   return a;
 }
 
+// Transform of L lines whose input is already in shared buffer a: every
+// pass goes shared -> shared (a, b alternating) except the last, which goes
+// to ``dst`` when LAST_TO_DST.  Returns the buffer holding the result
+// (meaningful when !LAST_TO_DST).
+template <bool LM, bool LAST_TO_DST, class Dst>
+__device__ double2 *fft_lines_smem(double2 *a, double2 *b, int N, int L, const int *rad, int np, int sgn,
+                                   const double2 *tw, const Dst &dst, int Ns0 = 1) {
+  int Ns = Ns0;
+  const int nin = LAST_TO_DST ? np - 1 : np;
+  for (int p = 0; p < nin; ++p) {
+    run_stream<LM>(rad[p], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, SmemDst<LM>{b, N, L});
+    __syncthreads();
+    double2 *t = a; a = b; b = t;
+    Ns *= rad[p];
+  }
+  if (LAST_TO_DST) run_stream<LM>(rad[np - 1], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, dst);
+  return a;
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(src));
+}
+__device__ __forceinline__ void cp_async8d(void *dst, const void *src) {
+  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit_wait() {
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_all;\n" ::);
+}
+
 // Lines per block and shared memory: two (lines x N) buffers when the
 // transform has a pass between two shared-memory stages, otherwise one, plus
 // the N twiddles; lines are capped so that a block stays within ~100 KB.
 __host__ __device__ __forceinline__ int fft_nbuf(int np, bool last_to_dst) {
-  const int smem_stages = last_to_dst ? np - 1 : np;   // passes that write shared memory
-  return smem_stages >= 2 ? 2 : 1;
+  // the copied-in tile plus one buffer per pass that writes shared memory,
+  // ping-ponging: two buffers unless the only pass streams straight out
+  const int smem_stages = last_to_dst ? np - 1 : np;
+  return smem_stages >= 1 ? 2 : 1;
 }
 __host__ __device__ __forceinline__ int fft_lines_per_block(int N, int nbuf, int cap) {
   int l = (100 * 1024) / (16 * N * nbuf);
@@ -254,46 +287,25 @@ __host__ __device__ __forceinline__ int fft_max_lines(int N, int nbuf) {
   return (200 * 1024) / (16 * N * nbuf) - 1;
 }
 __host__ __device__ __forceinline__ int fft_y_smem(const BoxDev &B) {
-  return (fft_nbuf(B.fft_y_np, false) * fft_y_pairs(B) + 1) * B.nym * 16;
+  // forward: lines + copied-in rows + twiddles; inverse: lines + raw
+  // half-spectrum rows (2 Pp (nym/2+1) complex) + twiddles
+  const int Pp = fft_y_pairs(B);
+  return ((2 * Pp + 1) * B.nym + 2 * Pp) * 16;
 }
 __host__ __device__ __forceinline__ int fft_z_smem(const BoxDev &B) {
   return (fft_nbuf(B.fft_z_np, true) * fft_z_lines(B) + 1) * B.nzm * 16;
 }
 
 // ---------------------------------------------------------------------------
-// y forward: rows (k, i) of length nym -> spec[k][i][ky], ky <= nym/2.  Two
-// real rows form one complex line.  FROM_VEL: the row values are the
-// divergence of (vx, vy, vz) times 1/(al dt) (CalcLocalDivergence.F90:28-38),
-// computed in the first pass; otherwise they are read from phi (dph).
+// y forward: rows (k, i) of length nym of dph -> spec[k][i][ky], ky <= nym/2.
 // ---------------------------------------------------------------------------
-template <bool FROM_VEL>
-struct YSrc {
-  const BoxDev *B;
-  int k, i0;
-  double usdtal, udx3m;
-  __device__ __forceinline__ double row(int i, int j) const {
-    if (i >= B->nzm) return 0.0;
-    const int N = B->nym, nzm = B->nzm;
-    const long long P = B->plane;
-    const long long o = (long long)k * P + (long long)i * N + j;
-    if (!FROM_VEL) return B->phi[o];
-    const int ip = i == nzm - 1 ? 0 : i + 1;
-    const int jp = j == N - 1 ? 0 : j + 1;
-    const double dq = (B->vz[(long long)k * P + (long long)ip * N + j] - B->vz[o]) * B->dz
-                    + (B->vy[(long long)k * P + (long long)i * N + jp] - B->vy[o]) * B->dy
-                    + (B->vx[o + P] - B->vx[o]) * udx3m;
-    return dq * usdtal;
-  }
-  __device__ __forceinline__ double2 operator()(int p, int j) const {
-    const int i = i0 + 2 * p;
-    return make_double2(row(i, j), row(i + 1, j));
-  }
-};
 struct NoDst {
   __device__ __forceinline__ void operator()(int, int, double2) const {}
 };
 
-template <bool FROM_VEL>
+// y forward over the rows of dph (phi): the 2*Pp rows of the block are
+// copied into shared memory with cp.async, packed two by two as complex
+// lines, transformed, and unpacked into the half spectrum.
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
@@ -307,14 +319,25 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / groups;
   const int i0 = (tile - k * groups) * 2 * Pp;
-  const int nb = fft_nbuf(B.fft_y_np, false);
-  double2 *a = fsm, *bb = fsm + (nb - 1) * Pp * N, *tws = fsm + nb * Pp * N;
+  double2 *a = fsm, *bb = fsm + Pp * N, *tws = fsm + 2 * Pp * N;
+  // copy in: row r of the block (i = i0 + r) as doubles into bb; line p is
+  // the complex pair (row 2p, row 2p+1), re-read below as double2 from a
+  double *rows = (double *)bb;
+  const double *phik = B.phi + (long long)k * B.plane;
+  for (int t = threadIdx.x; t < 2 * Pp * N; t += FFT_T) {
+    const int r = t / N, j = t - r * N;
+    if (i0 + r < nzm) cp_async8d(rows + r * N + j, phik + (long long)(i0 + r) * N + j);
+    else rows[r * N + j] = 0.0;
+  }
   for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twy + t);
+  cp_async_commit_wait();
   __syncthreads();
-  YSrc<FROM_VEL> src{&B, k, i0, FROM_VEL ? 1.0 / (S->dt * S->al) : 0.0,
-                     FROM_VEL ? tabk(B, T_UDX3M, k) : 0.0};
-  a = fft_lines<true, false>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, tws, src, NoDst{});
+  for (int t = threadIdx.x; t < Pp * N; t += FFT_T) {
+    const int p = t / N, j = t - p * N;
+    a[p * N + j] = make_double2(rows[2 * p * N + j], rows[(2 * p + 1) * N + j]);
+  }
   __syncthreads();
+  a = fft_lines_smem<true, false>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, tws, NoDst{});
   // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
   // B = (Z_q - conj Z_{N-q}) / (2i)
   const int nh = B.nymh;
@@ -367,11 +390,17 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn
   const int ky0 = (tile - k * ntl) * L;
   const int nb = fft_nbuf(B.fft_z_np, true);
   double2 *a = fsm, *bb = fsm + (nb - 1) * L * N, *tws = fsm + nb * L * N;
-  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twz + t);
-  __syncthreads();
   double2 *spec = B.spec + (long long)k * N * nh;
-  fft_lines<false, true>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, tws, ZSrc{spec, nh, ky0},
-                         ZDst{spec, nh, ky0, (double)(B.nzm * B.nym), sgn < 0});
+  for (int t = threadIdx.x; t < L * N; t += FFT_T) {
+    const int l = t % L, n = t / L;
+    if (ky0 + l < nh) cp_async16(a + n * L + l, spec + (long long)n * nh + ky0 + l);
+    else a[n * L + l] = make_double2(0.0, 0.0);
+  }
+  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twz + t);
+  cp_async_commit_wait();
+  __syncthreads();
+  fft_lines_smem<false, true>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, tws,
+                              ZDst{spec, nh, ky0, (double)(B.nzm * B.nym), sgn < 0});
 }
 
 // ---------------------------------------------------------------------------
@@ -383,6 +412,8 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn
 // applied to both parts.  The (0,0) mode is singular (Neumann in x): its
 // last equation is dropped and its last unknown set to zero.
 // ---------------------------------------------------------------------------
+constexpr int KP_U = 4;   // planes per prefetch chunk of the sweeps
+
 __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
@@ -398,30 +429,38 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
   const double *amph = B.tab + (long long)T_AMPHK * B.nx;
   const double *acph = B.tab + (long long)T_ACPHK * B.nx;
   const double *apph = B.tab + (long long)T_APPHK * B.nx;
-  double2 *x = B.spec + m;
-  double *dst = B.dstore + m;
+  double2 *__restrict__ x = B.spec + m;
+  double *__restrict__ dst = B.dstore + m;
   const long long st = nmode;
   const bool zero_mode = (ky == 0 && kz == 0);
-  // forward elimination
-  double s = 1.0 / ((__ldg(acph) - ak) - ak1);
-  double d = 1.0;
-  double2 y = x[0];
-  y.x = y.x * s; y.y = y.y * s;
-  double ap_prev = __ldg(apph) * s;
-  x[0] = y;
-  dst[0] = d;
-  for (int k = 1; k < nxm; ++k) {
-    s = 1.0 / ((__ldg(acph + k) - ak) - ak1);
-    const double am = __ldg(amph + k) * s;
-    const double fact = am / d;
-    d = 1.0 - fact * ap_prev;
-    double2 r = x[(long long)k * st];
-    r.x = r.x * s; r.y = r.y * s;
-    y.x = r.x - fact * y.x;
-    y.y = r.y - fact * y.y;
-    x[(long long)k * st] = y;
-    dst[(long long)k * st] = d;
-    ap_prev = __ldg(apph + k) * s;
+  // forward elimination (dgttrf + dgttrs forward sweep), planes in chunks
+  double d = 1.0, ap_prev = 0.0;
+  double2 y = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < nxm; k0 += KP_U) {
+    double2 r[KP_U];
+#pragma unroll
+    for (int u = 0; u < KP_U; ++u)
+      if (k0 + u < nxm) r[u] = x[(long long)(k0 + u) * st];
+#pragma unroll
+    for (int u = 0; u < KP_U; ++u) {
+      const int k = k0 + u;
+      if (k >= nxm) break;
+      const double s = 1.0 / ((__ldg(acph + k) - ak) - ak1);
+      double2 rk = r[u];
+      rk.x = rk.x * s; rk.y = rk.y * s;
+      if (k == 0) {
+        y = rk;
+      } else {
+        const double am = __ldg(amph + k) * s;
+        const double fact = am / d;
+        d = 1.0 - fact * ap_prev;
+        y.x = rk.x - fact * y.x;
+        y.y = rk.y - fact * y.y;
+      }
+      x[(long long)k * st] = y;
+      dst[(long long)k * st] = d;
+      ap_prev = __ldg(apph + k) * s;
+    }
   }
   // back substitution
   double2 xn;
@@ -432,36 +471,38 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
     xn.y = y.y / d;
   }
   x[(long long)(nxm - 1) * st] = xn;
-  for (int k = nxm - 2; k >= 0; --k) {
-    const double sk = 1.0 / ((__ldg(acph + k) - ak) - ak1);
-    const double ap = __ldg(apph + k) * sk;
-    const double dk = dst[(long long)k * st];
-    const double2 yk = x[(long long)k * st];
-    xn.x = (yk.x - ap * xn.x) / dk;
-    xn.y = (yk.y - ap * xn.y) / dk;
-    x[(long long)k * st] = xn;
+  for (int k0 = nxm - 2; k0 >= 0; k0 -= KP_U) {
+    double2 yk[KP_U];
+    double dk[KP_U];
+#pragma unroll
+    for (int u = 0; u < KP_U; ++u) {
+      const int k = k0 - u;
+      if (k >= 0) { yk[u] = x[(long long)k * st]; dk[u] = dst[(long long)k * st]; }
+    }
+#pragma unroll
+    for (int u = 0; u < KP_U; ++u) {
+      const int k = k0 - u;
+      if (k < 0) break;
+      const double sk = 1.0 / ((__ldg(acph + k) - ak) - ak1);
+      const double ap = __ldg(apph + k) * sk;
+      xn.x = (yk[u].x - ap * xn.x) / dk[u];
+      xn.y = (yk[u].y - ap * xn.y) / dk[u];
+      x[(long long)k * st] = xn;
+    }
   }
 }
 
-// ---------------------------------------------------------------------------
-// y inverse (complex-to-real, unnormalised): spec[k][i][ky] -> phi[k][i][j].
-// As in a c2r transform, the imaginary parts of the ky = 0 and ky = nym/2
-// coefficients are ignored.  Two rows are recovered from one complex line
-// Z = A + i B.
-// ---------------------------------------------------------------------------
-struct YInvSrc {
-  const double2 *spec; int N, nh, nzm, i0; bool even;
-  __device__ __forceinline__ double2 coef(int i, int n) const {
-    if (i >= nzm) return make_double2(0.0, 0.0);
+struct YInvSmemSrc {
+  const double2 *raw; int N, nh; bool even;    // raw: [row][nh] for the block's 2*Pp rows
+  __device__ __forceinline__ double2 coef(int r, int n) const {
     const int q = n < nh ? n : N - n;
-    double2 c = spec[(long long)i * nh + q];
+    double2 c = raw[r * nh + q];
     if (q == 0 || (even && 2 * q == N)) c.y = 0.0;
     else if (n >= nh) c.y = -c.y;
     return c;
   }
   __device__ __forceinline__ double2 operator()(int p, int n) const {
-    const int i = i0 + 2 * p;
-    const double2 A = coef(i, n), Bv = coef(i + 1, n);
+    const double2 A = coef(2 * p, n), Bv = coef(2 * p + 1, n);
     return make_double2(A.x - Bv.y, A.y + Bv.x);
   }
 };
@@ -474,6 +515,12 @@ struct YInvDst {
   }
 };
 
+// y inverse (complex-to-real, unnormalised): spec[k][i][ky] -> phi[k][i][j].
+// As in a c2r transform, the imaginary parts of the ky = 0 and ky = nym/2
+// coefficients are ignored.  The block's half-spectrum rows are copied into
+// shared memory with cp.async; two rows are recovered from one complex line
+// Z = A + i B.  The raw rows' buffer becomes the second ping-pong buffer once
+// the first pass has read it.
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns) {
   extern __shared__ double2 fsm[];
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
@@ -486,13 +533,27 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns) {
   const int tile = blockIdx.x - __ldg(bt.tile_off + b);
   const int k = tile / groups;
   const int i0 = (tile - k * groups) * 2 * Pp;
-  const int nb = fft_nbuf(B.fft_y_np, true);
-  double2 *a = fsm, *bb = fsm + (nb - 1) * Pp * N, *tws = fsm + nb * Pp * N;
+  // layout: a = Pp*N, raw (= b) = 2*Pp*nh >= Pp*N, twiddles
+  double2 *a = fsm, *raw = fsm + Pp * N, *tws = raw + 2 * Pp * nh;
+  const double2 *speck = B.spec + (long long)k * nzm * nh;
+  for (int t = threadIdx.x; t < 2 * Pp * nh; t += FFT_T) {
+    const int r = t / nh, q = t - r * nh;
+    if (i0 + r < nzm) cp_async16(raw + t, speck + (long long)(i0 + r) * nh + q);
+    else raw[t] = make_double2(0.0, 0.0);
+  }
   for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twy + t);
+  cp_async_commit_wait();
   __syncthreads();
-  fft_lines<true, true>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, +1, tws,
-                        YInvSrc{B.spec + (long long)k * nzm * nh, N, nh, nzm, i0, (N % 2) == 0},
-                        YInvDst{B.phi + (long long)k * B.plane, N, nzm, i0});
+  const int np = B.fft_y_np;
+  YInvDst dst{B.phi + (long long)k * B.plane, N, nzm, i0};
+  const YInvSmemSrc src{raw, N, nh, (N % 2) == 0};
+  if (np == 1) {
+    run_stream<true>(B.fft_y_radix[0], N, Pp, 1, +1, tws, src, dst);
+    return;
+  }
+  run_stream<true>(B.fft_y_radix[0], N, Pp, 1, +1, tws, src, SmemDst<true>{a, N, Pp});
+  __syncthreads();
+  fft_lines_smem<true, true>(a, raw, N, Pp, B.fft_y_radix + 1, np - 1, +1, tws, dst, B.fft_y_radix[0]);
 }
 
 }  // namespace afid

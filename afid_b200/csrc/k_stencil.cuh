@@ -227,26 +227,13 @@ __global__ void k_substep_prep(const BoxDev *__restrict__ boxes, int nbox, int n
   }
 }
 
-// ---------------------------------------------------------------------------
-// K1: explicit terms + implicit rhs + forward elimination for all four
-// fields, one thread per (j, i) column marching k upwards.  A ring of four
-// x-planes of vx, vy, vz, temp, pr (tile + 1-cell halo) sits in shared
-// memory; plane kc+2 is fetched with cp.async while plane kc is computed.
-// Writes the RK history (rux.. = H) and the forward-sweep values y of each
-// solve; the temperature sweep starts from y(1) = 0 and the missing
-// contribution of its wall row is added by K2 (the solve is linear in y(1)).
-// ---------------------------------------------------------------------------
 constexpr int K1_TJ = 32;
 constexpr int K1_TI = 8;
 constexpr int K1_HJ = K1_TJ + 2;
 constexpr int K1_HI = K1_TI + 2;
 constexpr int K1_PL = K1_HJ * K1_HI;            // one halo plane of one field (340)
 constexpr int K1_NT = K1_TJ * K1_TI;            // threads per block (256)
-constexpr int K1_NSLOT = 4;
 constexpr int K1_NTAB = 14;                     // per-k scalars staged per plane
-constexpr int K1_RING = K1_NSLOT * F_NF * K1_PL;        // doubles
-constexpr int K1_TABR = K1_NSLOT * 16;                  // doubles
-constexpr int K1_SMEM = (K1_RING + K1_TABR) * 8;
 
 // per-k scalar slots staged in shared memory
 enum K1Tab { KT_UDX3M = 0, KT_UDX3C, KT_AM3SK, KT_AC3SK, KT_AP3SK, KT_AM3CK, KT_AC3CK, KT_AP3CK,
@@ -308,23 +295,33 @@ __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int 
 
 // ---------------------------------------------------------------------------
 // K1: explicit terms + implicit rhs + forward elimination for all four
-// fields, one thread per (j, i) column marching k upwards.  MINB is the
-// occupancy target (resident blocks per SM; 3 caps registers at 80, 2 at
-// 128).  Shared memory holds a ring of four x-planes of vx, vy, vz, temp, pr (tile plus a 1-cell
-// halo) and of the per-k metric and LU scalars; plane k+3 is fetched with
-// cp.async while plane k is computed, so each load has two planes of compute
-// to arrive in.  Plane k-1 is not read from the ring: the seven values of it
-// that the stencils need are kept in registers.  The RK history of plane k+2
-// is loaded into registers two planes ahead.  Writes the RK history (rux.. =
-// H) and the forward-sweep values y of each solve; the temperature sweep
-// starts from y(1) = 0 and the missing contribution of its wall row is added
-// by K2 (the solve is linear in y(1)).
+// fields, one thread per (j, i) column marching k upwards, PPB planes per
+// block barrier.  MINB is the occupancy target (resident blocks per SM; 3
+// caps registers at 80, 2 at 128).  Shared memory holds a ring of x-planes
+// of vx, vy, vz, temp, pr (tile plus a 1-cell halo) and of the per-k metric
+// and LU scalars, fetched with cp.async 2 PPB + 1 planes ahead so that each
+// load has two barrier intervals of compute to arrive in.  Plane k-1 is not
+// read from the ring: the seven values of it that the stencils need are kept
+// in registers.  The RK history of the next PPB planes is loaded into
+// registers one interval ahead.  Writes the RK history (rux.. = H) and the
+// forward-sweep values y of each solve; the temperature sweep starts from
+// y(1) = 0 and the missing contribution of its wall row is added by K2 (the
+// solve is linear in y(1)).
 // ---------------------------------------------------------------------------
-template <int MINB>
+template <int PPB>
+struct K1Ring {
+  static constexpr int D = 2 * PPB + 1;        // prefetch distance in planes
+  static constexpr int NS = D + PPB;           // ring slots
+  static constexpr int SMEM = (NS * F_NF * K1_PL + NS * 16) * 8;
+};
+
+template <int MINB, int PPB>
 __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev bt, int ns) {
+  constexpr int NS = K1Ring<PPB>::NS;
+  constexpr int D = K1Ring<PPB>::D;
   extern __shared__ double k1sm[];
   double *ring = k1sm;
-  double *tring = k1sm + K1_RING;            // [slot][16]
+  double *tring = k1sm + NS * F_NF * K1_PL;      // [slot][16]
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
@@ -366,17 +363,18 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
       g1 = (long long)ii * nym + jj;
     }
   }
-  auto load_plane = [&](int p) {      // plane p and its per-k scalars into slot p & 3
-    double *dst = ring + (p & (K1_NSLOT - 1)) * F_NF * K1_PL;
+  auto load_plane = [&](int p) {      // plane p and its per-k scalars into slot p % NS
+    if (p > nx - 1) return;
+    const int sl = p % NS;
+    double *dst = ring + sl * F_NF * K1_PL;
     const long long po = (long long)p * P;
 #pragma unroll
     for (int f = 0; f < F_NF; ++f) {
       cp_async8(dst + f * K1_PL + tid, fld[f] + po + g0);
       if (has1) cp_async8(dst + f * K1_PL + r1, fld[f] + po + g1);
     }
-    if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + (p & (K1_NSLOT - 1)) * 16 + tid, k1_tab_src(B, tid, p));
+    if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + sl * 16 + tid, k1_tab_src(B, tid, p));
   };
-  // RK history of a plane, straight into registers
   auto load_hist = [&](int p, double (&h)[4]) {
     if (inside && p <= nxm - 1) {
       const long long o = (long long)p * P + col;
@@ -392,86 +390,98 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
   // forward-sweep carries
   double yX = inside ? B.wall[col] : 0.0;   // rhs(1,j,i) left by the last vz solve
   double yY = 0.0, yZ = 0.0, yT = 0.0;
-  double h0[4] = {0.0, 0.0, 0.0, 0.0}, h1[4] = {0.0, 0.0, 0.0, 0.0}, h2[4] = {0.0, 0.0, 0.0, 0.0};
+  double hc[PPB][4], hn[PPB][4];
+#pragma unroll
+  for (int u = 0; u < PPB; ++u)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { hc[u][q] = 0.0; hn[u][q] = 0.0; }
 
-  load_plane(0);
-  load_plane(1);
+  for (int p = 0; p < D - PPB; ++p) load_plane(p);
   cp_async_commit();
-  if (2 <= nx - 1) load_plane(2);
+  for (int p = D - PPB; p < D; ++p) load_plane(p);
   cp_async_commit();
-  load_hist(0, h0);
-  load_hist(1, h1);
+#pragma unroll
+  for (int u = 0; u < PPB; ++u) load_hist(u, hc[u]);
   cp_async_wait_1();
   __syncthreads();
 
-  for (int kc = 0; kc < nxm; ++kc) {
-    if (kc + 3 <= nx - 1) load_plane(kc + 3);
+  for (int k0 = 0; k0 < nxm; k0 += PPB) {
+#pragma unroll
+    for (int u = 0; u < PPB; ++u) load_plane(k0 + D + u);
     cp_async_commit();
-    load_hist(kc + 2, h2);
-    acc.s_c = kc & 3;
-    acc.s_p = (kc + 1) & 3;
-    const double *tk = tring + (kc & 3) * 16;
-    if (inside) {
-      const long long o = (long long)kc * P + col;
-      const int dkm = kc == 0 ? 0 : -1;
-      const int dkp = kc == nxm - 1 ? 0 : 1;
-      const double udx3m_k = tk[KT_UDX3M];
-      const double am_s = tk[KT_AM3SK], ac_s = tk[KT_AC3SK], ap_s = tk[KT_AP3SK];
-      // vy, vz: rows kc = 0..nxm-1 of the size-nxm systems
-      {
-        const double H = h_vy(acc, c, udx3m_k, dkm, dkp);
-        const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
-        const double r = rhs_vyz(H, h0[1], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
-                                 acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
-        B.ruy[o] = H;
-        const double bb = r * tk[KT_YSC];
-        yY = (kc == 0) ? bb : bb - tk[KT_YF] * yY;
-        B.ybuf[1][o] = yY;
-      }
-      {
-        const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
-        const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
-        const double r = rhs_vyz(H, h0[2], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
-                                 acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
-        B.ruz[o] = H;
-        const double bb = r * tk[KT_YSC];
-        yZ = (kc == 0) ? bb : bb - tk[KT_YF] * yZ;
-        B.ybuf[2][o] = yZ;
-      }
-      if (kc >= 1) {
-        const double udx3c_k = tk[KT_UDX3C];
-        const double am_c = tk[KT_AM3CK], ac_c = tk[KT_AC3CK], ap_c = tk[KT_AP3CK];
+#pragma unroll
+    for (int u = 0; u < PPB; ++u) load_hist(k0 + PPB + u, hn[u]);
+#pragma unroll
+    for (int u = 0; u < PPB; ++u) {
+      const int kc = k0 + u;
+      if (kc >= nxm) break;
+      acc.s_c = kc % NS;
+      acc.s_p = (kc + 1) % NS;
+      const double *tk = tring + (kc % NS) * 16;
+      if (inside) {
+        const long long o = (long long)kc * P + col;
+        const int dkm = kc == 0 ? 0 : -1;
+        const int dkp = kc == nxm - 1 ? 0 : 1;
+        const double udx3m_k = tk[KT_UDX3M];
+        const double am_s = tk[KT_AM3SK], ac_s = tk[KT_AC3SK], ap_s = tk[KT_AP3SK];
+        // vy, vz: rows kc = 0..nxm-1 of the size-nxm systems
         {
-          const double H = h_vx(acc, c, udx3c_k);
-          const double r = rhs_vx(H, h0[0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
-                                  acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
-                                  am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
-          B.rux[o] = H;
-          const double bb = r * tk[KT_XSC];
-          yX = bb - tk[KT_XF] * yX;
-          B.ybuf[0][o] = yX;
+          const double H = h_vy(acc, c, udx3m_k, dkm, dkp);
+          const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
+          const double r = rhs_vyz(H, hc[u][1], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
+                                   acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
+          B.ruy[o] = H;
+          const double bb = r * tk[KT_YSC];
+          yY = (kc == 0) ? bb : bb - tk[KT_YF] * yY;
+          B.ybuf[1][o] = yY;
         }
         {
-          const double H = h_temp(acc, c, udx3c_k);
-          const double r = rhs_temp(H, h0[3], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
-                                    acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
-          B.rutemp[o] = H;
-          const double bb = r * tk[KT_TSC];
-          yT = bb - tk[KT_TF] * yT;
-          B.ybuf[3][o] = yT;
+          const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
+          const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
+          const double r = rhs_vyz(H, hc[u][2], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
+                                   acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
+          B.ruz[o] = H;
+          const double bb = r * tk[KT_YSC];
+          yZ = (kc == 0) ? bb : bb - tk[KT_YF] * yZ;
+          B.ybuf[2][o] = yZ;
         }
+        if (kc >= 1) {
+          const double udx3c_k = tk[KT_UDX3C];
+          const double am_c = tk[KT_AM3CK], ac_c = tk[KT_AC3CK], ap_c = tk[KT_AP3CK];
+          {
+            const double H = h_vx(acc, c, udx3c_k);
+            const double r = rhs_vx(H, hc[u][0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
+                                    acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
+                                    am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
+            B.rux[o] = H;
+            const double bb = r * tk[KT_XSC];
+            yX = bb - tk[KT_XF] * yX;
+            B.ybuf[0][o] = yX;
+          }
+          {
+            const double H = h_temp(acc, c, udx3c_k);
+            const double r = rhs_temp(H, hc[u][3], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
+                                      acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
+            B.rutemp[o] = H;
+            const double bb = r * tk[KT_TSC];
+            yT = bb - tk[KT_TF] * yT;
+            B.ybuf[3][o] = yT;
+          }
+        }
+        // stash what plane kc+1 will need of this plane
+        acc.prev.vx = acc(F_VX, 0, 0, 0);
+        acc.prev.vy = acc(F_VY, 0, 0, 0);
+        acc.prev.vy_jp = acc(F_VY, 0, 1, 0);
+        acc.prev.vz = acc(F_VZ, 0, 0, 0);
+        acc.prev.vz_ip = acc(F_VZ, 0, 0, 1);
+        acc.prev.t = acc(F_T, 0, 0, 0);
+        acc.prev.pr = acc(F_PR, 0, 0, 0);
       }
-      // stash what plane kc+1 will need of this plane
-      acc.prev.vx = acc(F_VX, 0, 0, 0);
-      acc.prev.vy = acc(F_VY, 0, 0, 0);
-      acc.prev.vy_jp = acc(F_VY, 0, 1, 0);
-      acc.prev.vz = acc(F_VZ, 0, 0, 0);
-      acc.prev.vz_ip = acc(F_VZ, 0, 0, 1);
-      acc.prev.t = acc(F_T, 0, 0, 0);
-      acc.prev.pr = acc(F_PR, 0, 0, 0);
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) { h0[q] = h1[q]; h1[q] = h2[q]; }
+    for (int u = 0; u < PPB; ++u)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) hc[u][q] = hn[u][q];
     cp_async_wait_1();
     __syncthreads();
   }
@@ -485,7 +495,7 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
 // ---------------------------------------------------------------------------
 constexpr int K2_U = 4;   // planes loaded per chunk (loads of a chunk are all in flight together)
 
-__global__ void __launch_bounds__(256) k_implicit_bwd(BatchDev bt, int ns) {
+__global__ void __launch_bounds__(256, 3) k_implicit_bwd(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
@@ -663,20 +673,52 @@ __device__ __forceinline__ double local_div(const BoxDev &B, int k, int j, int i
        + (B.vx[o + P] - B.vx[o]) * tabk(B, T_UDX3M, k);
 }
 
-__global__ void __launch_bounds__(256) k_divergence(BatchDev bt) {
+// Column march: one thread per (j, i), planes in chunks whose loads are all
+// in flight together; vx(k+1) of one plane is vx(k) of the next.
+constexpr int KD_U = 4;
+__global__ void __launch_bounds__(256, 3) k_divergence(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
-  if (!B.active) return;
+  if (!B.active || ns >= B.nsst) return;
   const BoxScalars *S = B.sc;
-  const long long cell = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
+  if (S->status != 0) return;
+  const long long col = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
   const long long P = B.plane;
-  if (cell >= (long long)B.nxm * P) return;
-  const int k = (int)(cell / P);
-  const long long col = cell - (long long)k * P;
-  const int i = (int)(col / B.nym);
-  const int j = (int)(col - (long long)i * B.nym);
+  if (col >= P) return;
+  const int nym = B.nym, nzm = B.nzm, nxm = B.nxm;
+  const int i = (int)(col / nym);
+  const int j = (int)(col - (long long)i * nym);
+  const long long oip = (long long)(i == nzm - 1 ? 0 : i + 1) * nym + j - col;
+  const long long ojp = (long long)i * nym + (j == nym - 1 ? 0 : j + 1) - col;
+  const double *__restrict__ vx = B.vx + col;
+  const double *__restrict__ vy = B.vy + col;
+  const double *__restrict__ vz = B.vz + col;
+  double *__restrict__ phi = B.phi + col;
   const double usdtal = 1.0 / (S->dt * S->al);
-  B.phi[cell] = local_div(B, k, j, i) * usdtal;
+  const double dz = B.dz, dy = B.dy;
+  double xk = vx[0];
+  for (int k0 = 0; k0 < nxm; k0 += KD_U) {
+    double zc[KD_U], zp[KD_U], yc[KD_U], yp[KD_U], xn[KD_U];
+#pragma unroll
+    for (int u = 0; u < KD_U; ++u) {
+      const int k = k0 + u;
+      if (k < nxm) {
+        const long long o = (long long)k * P;
+        zc[u] = vz[o]; zp[u] = vz[o + oip];
+        yc[u] = vy[o]; yp[u] = vy[o + ojp];
+        xn[u] = vx[o + P];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < KD_U; ++u) {
+      const int k = k0 + u;
+      if (k >= nxm) break;
+      // CalcLocalDivergence.F90:34-37
+      const double dq = (zp[u] - zc[u]) * dz + (yp[u] - yc[u]) * dy + (xn[u] - xk) * tabk(B, T_UDX3M, k);
+      phi[(long long)k * P] = dq * usdtal;
+      xk = xn[u];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -15,9 +15,9 @@ With N > 1 (torchrun) every rank advances its own replica of the workload
 (the path does not shard a box across GPUs; ensemble boxes are independent),
 and the time is the maximum over ranks.
 
-``--impl reference`` times the CPU restatement of the reference (the
-oracle, NumPy/SciPy) on a bounded sample of the same workload on the host
-cores; the Fortran reference cannot be built in this image.
+``--impl reference`` times the C/OpenMP restatement of the reference
+(oracle/afid_cpu.c, all host threads) on a bounded sample of the same
+workload; the Fortran reference cannot be built in this image.
 """
 from __future__ import annotations
 
@@ -45,7 +45,7 @@ UNIT = "Mpoint-steps/s"
 # (traffic scales with the number of cells; the kernels have the same
 # per-cell structure at every size).
 NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
-    "explicit_fwd": 135.8, "implicit_bwd": 94.5, "fft_y_fwd": 31.8, "fft_z_fwd": 14.3,
+    "explicit_fwd": 135.8, "implicit_bwd": 94.5, "fft_z_fwd": 14.3,
     "poisson_x": 34.0, "fft_z_inv": 14.3, "fft_y_inv": 14.6,
 }
 
@@ -90,7 +90,8 @@ def kernel_bytes_per_cell(cfg) -> dict[str, float]:
     return {
         "explicit_fwd": 17 * 8.0,   # R vx vy vz temp pr rux ruy ruz rutemp, W rux ruy ruz rutemp + 4 sweeps
         "implicit_bwd": 12 * 8.0,   # R 4 sweeps + vx vy vz temp, W vx vy vz temp
-        "fft_y_fwd": 24.0 + spec,   # R vx vy vz, W spectrum
+        "divergence": 32.0,         # R vx vy vz, W dph
+        "fft_y_fwd": 8.0 + spec,    # R dph, W spectrum
         "fft_z_fwd": 2 * spec,
         "poisson_x": 2 * spec,
         "fft_z_inv": 2 * spec,
@@ -188,26 +189,36 @@ def cpu_sample_cfg(workload: str):
     nxm = {"c2": 384, "c3": 512, "s384": 192}[workload]
     ra = {"c2": 1e9, "c3": 1e10, "s384": 1e9}[workload]
     dt = {"c2": 1e-4, "c3": 5e-5, "s384": 1e-4}[workload]
-    return BouIn(nxm=nxm, nym=48, nzm=48, ylen=2.0 * 48 / 768, zlen=2.0 * 48 / 768, ray=ra, dt=dt,
-                 istr3=7), f"a {nxm + 1}x48x48 column of the workload (same x grid, Ra, dt)"
+    return BouIn(nxm=nxm, nym=96, nzm=96, ylen=2.0 * 96 / 768, zlen=2.0 * 96 / 768, ray=ra, dt=dt,
+                 istr3=7), f"a {nxm + 1}x96x96 column of the workload (same x grid, Ra, dt)"
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def run_oracle_sample(workload: str, steps: int, warmup: int):
-    """Returns (Mpoint-steps/s, seconds per step, sample description)."""
+    """The compiled C restatement (oracle/afid_cpu.c, OpenMP over all host
+    threads) on a bounded sample of the workload.
+    Returns (Mpoint-steps/s, seconds per step, sample description, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle import afid_oracle as O
     from helpers import oracle_state
+    from oracle.cpu_port import CpuBox
     cfg, desc = cpu_sample_cfg(workload)
     s = oracle_state(cfg, seed=0)
-    for _ in range(warmup):
-        O.time_marcher(s, cfg.dt, vectorised_poisson=True)
+    box = CpuBox(cfg, s.g.xc)
+    for f in ("vx", "vy", "vz", "temp", "pr"):
+        box.set(f, getattr(s, f))
+    if warmup:
+        box.step(cfg.dt, warmup)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        O.calc_max_cfl(s)
-        O.time_marcher(s, cfg.dt, vectorised_poisson=True)
-        O.calc_plate_nu(s)
+    box.step(cfg.dt, steps)
     t = time.perf_counter() - t0
-    return cells(cfg) * steps / t / 1e6, t / steps, desc
+    box.close()
+    return cells(cfg) * steps / t / 1e6, t / steps, desc, cpu_threads()
 
 
 def reference_arm(args):
@@ -216,7 +227,7 @@ def reference_arm(args):
         return 0
     boxes, conf = workload_boxes(args.workload)
     steps = max(1, args.steps)
-    val, tps, desc = run_oracle_sample(args.workload, steps, max(0, min(args.warmup, 1)))
+    val, tps, desc, thr = run_oracle_sample(args.workload, steps, max(0, min(args.warmup, 1)))
     conf = dict(conf)
     conf["cpu_sample"] = desc
     line = {
@@ -224,10 +235,10 @@ def reference_arm(args):
         "warmup": args.warmup, "ms_per_step": tps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": conf, "impl": "reference",
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"{steps} RK3 steps of {desc}; NumPy/SciPy oracle (single-threaded "
-                                   "NumPy, LAPACK through SciPy); the Fortran reference has no "
-                                   "compiler in this image"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": f"{steps} RK3 steps of {desc} with the C/OpenMP restatement of "
+                                   "the reference (oracle/afid_cpu.c, checked against the NumPy "
+                                   "oracle); the Fortran reference has no compiler in this image"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -390,10 +401,10 @@ def gpu_arm(args):
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if world == 1 and not args.no_cpu:
-        v, tps, desc = run_oracle_sample(args.workload, steps=3, warmup=1)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"3 RK3 steps of {desc} with the NumPy/SciPy oracle "
-                         f"({tps:.2f} s/step, single-threaded NumPy)"}
+        v, tps, desc, thr = run_oracle_sample(args.workload, steps=5, warmup=1)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"5 RK3 steps of {desc} with the C/OpenMP restatement of the reference "
+                         f"(oracle/afid_cpu.c, {tps:.2f} s/step on {thr} host threads)"}
 
     if rank == 0:
         conf = dict(conf)

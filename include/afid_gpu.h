@@ -123,8 +123,10 @@ int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
 int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
 /* Launch-shape tuning of one box (no counterpart in the reference):
  * row pairs per y-FFT block, ky columns per z-FFT block (0 = built-in
- * choice) and the resident-block target of the explicit/forward kernel
- * (2 or 3; 0 = 2).  Results do not depend on these values. */
+ * choice) and the variant of the explicit/forward kernel: 2 = two resident
+ * blocks per SM, one plane per barrier; 3 = three resident blocks; 4 = two
+ * resident blocks, two planes per barrier (0 = 2).  Results do not depend on
+ * these values. */
 int afid_box_set_tuning(afid_ctx *ctx, int box_id, int fft_y_lines, int fft_z_lines, int k1_minb);
 /* Copies up to max_records of the most recent per-step records, oldest
  * first; returns the number copied (>= 0) or an error code. */
@@ -168,14 +170,15 @@ enum afid_kernel {
   AFID_K_PREP = 2,          /* substep coefficients and x-tridiagonal LU */
   AFID_K_EXPLICIT_FWD = 3,  /* ExplicitTerms* + ImplicitAndUpdate* rhs + forward sweeps */
   AFID_K_IMPLICIT_BWD = 4,  /* back substitution + update of vx, vy, vz, temp */
-  AFID_K_FFT_Y_FWD = 5,     /* CalcLocalDivergence + r2c along y */
+  AFID_K_FFT_Y_FWD = 5,     /* r2c along y */
   AFID_K_FFT_Z_FWD = 6,     /* c2c along z, forward */
   AFID_K_POISSON_X = 7,     /* complex tridiagonal per (ky, kz) */
   AFID_K_FFT_Z_INV = 8,     /* c2c along z, backward */
   AFID_K_FFT_Y_INV = 9,     /* c2r along y into dph */
   AFID_K_CORRECT = 10,      /* CorrectVelocity + CorrectPressure */
   AFID_K_PLATE_NU = 11,     /* CalcPlateNu partial sums */
-  AFID_K_COUNT = 12
+  AFID_K_DIVERGENCE = 12,   /* CalcLocalDivergence */
+  AFID_K_COUNT = 13
 };
 /* afid_step with a CUDA event after every launch: adds each kernel's
  * device time (ms) into kernel_ms[slot] and its launch count into

@@ -28,7 +28,7 @@ def test_candidates_fit_shared_memory(nyz):
         assert (2 * v + 1) * nyz * 16 <= 200 * 1024
     for v in c["fft_z_lines"]:
         assert (2 * v + 1) * nyz * 16 <= 200 * 1024 and v <= nyz // 2 + 1
-    assert c["k1_minb"] == [2, 3]
+    assert c["k1_minb"] == [2, 3, 4]
 
 
 def test_cache_roundtrip(tmp_path):
