@@ -41,22 +41,25 @@ def fft_plan(n: int) -> list[int]:
             m //= p
     if m != 1:
         raise ValueError(f"{n}: prime factor > 7")
-    return sorted(rad)
+    return rad
 
 
-def _nbuf(np_: int, last_to_dst: bool) -> int:
-    stages = np_ - 1 if last_to_dst else np_
-    return 2 if stages >= 1 else 1
+SMEM_MAX = 200 * 1024   # shared memory of one transform block (two copy-in slots, twiddles)
+TILE_MAX = 14 * 256     # complex values of one in-place tile
 
 
-def _max_lines(n: int, nbuf: int) -> int:
-    return (200 * 1024) // (16 * n * nbuf) - 1
+def fft_y_bytes(n: int, pairs: int) -> int:
+    return (2 * 2 * pairs * (n // 2 + 1) + n) * 16
+
+
+def fft_z_bytes(n: int, lines: int) -> int:
+    return (2 * lines * n + n) * 16
 
 
 def candidates(cfg: BouIn) -> dict:
-    ny = [v for v in (1, 2, 4, 8, 16) if v <= _max_lines(cfg.nym, _nbuf(len(fft_plan(cfg.nym)), False))]
-    nz_max = min(_max_lines(cfg.nzm, _nbuf(len(fft_plan(cfg.nzm)), True)), cfg.nym // 2 + 1)
-    nz = [v for v in (1, 2, 4, 8, 16, 32) if v <= nz_max]
+    ny = [v for v in (1, 2, 4, 8, 16) if fft_y_bytes(cfg.nym, v) <= SMEM_MAX and v * cfg.nym <= TILE_MAX]
+    nz = [v for v in (1, 2, 4, 8, 16) if fft_z_bytes(cfg.nzm, v) <= SMEM_MAX and v * cfg.nzm <= TILE_MAX
+          and v < 2 * (cfg.nym // 2 + 1)]
     return {"fft_y_lines": ny or [1], "fft_z_lines": nz or [1], "k1_minb": [2, 3, 4]}
 
 

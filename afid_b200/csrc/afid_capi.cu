@@ -1,5 +1,6 @@
 // Host side of libafid_gpu: contexts, boxes, metric tables, batches, launch
 // sequences and the C-ABI of include/afid_gpu.h.
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdarg>
@@ -64,6 +65,8 @@ struct Batch {
   int *d_off = nullptr;     // NFAM x (nbox + 1)
   int total[NFAM] = {};
   size_t smem_y = 0, smem_z = 0;
+  FftSmem sm_y{0}, sm_z{0};         // slot sizes of the persistent transforms
+  int grid_y = 0, grid_z = 0;       // their resident grids
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
   int k1_minb = 2;          // variant of the explicit/forward kernel (tuning, 2..4)
@@ -72,8 +75,9 @@ struct Batch {
 long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
 
 // FFT plan of length n: radix 16 for every four factors of two, one radix
-// 8, 4 or 2 for the rest, then 3, 5 and 7; passes in increasing radix order
-// so that the large radices run last, in place, with few butterflies.
+// 8, 4 or 2 for the rest, then 3, 5 and 7.  The power-of-two passes come
+// first, so that the stride Ns of every pass but those after a second odd
+// radix is a power of two (shift and mask indexing).
 int factor_radices(int n, int *rad, int *np) {
   int m = n, a = 0, c = 0;
   while (m % 2 == 0) { m /= 2; ++a; }
@@ -84,9 +88,6 @@ int factor_radices(int n, int *rad, int *np) {
   for (int q = 0; q < 3; ++q)
     while (m % odd[q] == 0 && c < 15) { tmp[c++] = odd[q]; m /= odd[q]; }
   if (m != 1 || c > 15 || c == 0) return -1;
-  // insertion sort, increasing
-  for (int x = 1; x < c; ++x)
-    for (int y = x; y > 0 && tmp[y - 1] > tmp[y]; --y) { int t = tmp[y]; tmp[y] = tmp[y - 1]; tmp[y - 1] = t; }
   for (int x = 0; x < c; ++x) rad[x] = tmp[x];
   rad[c] = 0;
   *np = c;
@@ -98,7 +99,7 @@ long long tiles_of(const BoxDev &B, int fam) {
     case FAM_K1: return cdiv(B.nym, K1_TJ) * cdiv(B.nzm, K1_TI);
     case FAM_COL: return cdiv(B.plane, 256);
     case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
-    case FAM_DIAG: return cdiv((long long)B.nxm * B.plane, 1024);
+    case FAM_DIAG: return cdiv(B.plane, 256);
     case FAM_FY: return (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
     case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
     case FAM_PX: return cdiv((long long)B.nzm * B.nymh, 256);
@@ -262,6 +263,30 @@ int get_box(afid_ctx *c, int id, HostBox **out) {
   return 0;
 }
 
+int init_kernel_attrs();
+
+// slot sizes (complex values) and twiddle lengths of the persistent
+// transforms, grown to cover box d
+void fft_smem_grow(const BoxDev &d, FftSmem &y, FftSmem &z, int &twy, int &twz) {
+  const int Pp = fft_y_pairs(d), L = fft_z_lines(d);
+  y.slot = std::max(y.slot, fft_y_slot(d.nym, Pp));
+  z.slot = std::max(z.slot, L * d.nzm);
+  twy = std::max(twy, d.nym);
+  twz = std::max(twz, d.nzm);
+}
+
+// resident grid of a persistent transform: SMs x blocks per SM, at most tiles
+template <class K>
+int fft_grid(K kernel, size_t smem, int tiles, int *grid) {
+  int dev = 0, nsm = 0, occ = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, FFT_T, smem));
+  if (occ < 1) return fail(AFID_ESIZE, "transform block of %zu bytes of shared memory does not fit an SM", smem);
+  *grid = std::max(1, std::min(tiles, nsm * occ));
+  return 0;
+}
+
 int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   if (n <= 0 || !ids) return fail(AFID_EINVAL, "empty box set");
   std::vector<int> key(ids, ids + n);
@@ -270,6 +295,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   std::vector<BoxDev> devs;
   std::vector<int> off((size_t)NFAM * (n + 1), 0);
   Batch *bt = new Batch();
+  int twy_max = 0, twz_max = 0;
   bt->ids = key;
   for (int b = 0; b < n; ++b) {
     HostBox *hb;
@@ -278,11 +304,10 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     BoxDev d = hb->dev;
     d.active = 1;
     devs.push_back(d);
-    const size_t sy = (size_t)fft_y_smem(d);
-    const size_t sz = (size_t)fft_z_smem(d);
-    if (sy > bt->smem_y) bt->smem_y = sy;
-    if (sz > bt->smem_z) bt->smem_z = sz;
+    fft_smem_grow(d, bt->sm_y, bt->sm_z, twy_max, twz_max);
   }
+  bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16;
+  bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16;
   for (int f = 0; f < NFAM; ++f) {
     long long acc = 0;
     for (int b = 0; b < n; ++b) {
@@ -300,6 +325,12 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   }
   CK(cudaMemcpy(bt->d_boxes, devs.data(), sizeof(BoxDev) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(bt->d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+  {
+    int rc = init_kernel_attrs();
+    if (!rc) rc = fft_grid(k_fft_y_fwd, bt->smem_y, bt->total[FAM_FY], &bt->grid_y);
+    if (!rc) rc = fft_grid(k_fft_z, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
+    if (rc) { free_batch(bt); return rc; }
+  }
   {
     long long w[5] = {0, 0, 0, 0, 0};
     for (const BoxDev &d : devs) w[d.k1_minb >= 2 && d.k1_minb <= 4 ? d.k1_minb : 2] += d.fsize;
@@ -328,7 +359,7 @@ int init_kernel_attrs() {
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1>::SMEM));
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1>::SMEM));
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<2>::SMEM));
-  const int fsm = 200 * 1024;   // lines x N plus twiddles, bounded by the nym, nzm <= 8192 limit
+  const int fsm = FFT_SMEM_MAX;   // two slots + work + twiddles: (4 N + 4) 16 bytes at one line
   CK(cudaFuncSetAttribute(k_fft_y_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
@@ -367,19 +398,19 @@ int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof 
     CKL();
     PMARK(pf, AFID_K_DIVERGENCE);
   }
-  k_fft_y_fwd<<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
+  k_fft_y_fwd<<<bt->grid_y, FFT_T, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns, bt->sm_y, bt->total[FAM_FY]);
   CKL();
   PMARK(pf, AFID_K_FFT_Y_FWD);
-  k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, -1);
+  k_fft_z<<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, -1, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
   PMARK(pf, AFID_K_FFT_Z_FWD);
   k_poisson_x<<<bt->total[FAM_PX], 256, 0, s>>>(bdev(bt, FAM_PX), ns);
   CKL();
   PMARK(pf, AFID_K_POISSON_X);
-  k_fft_z<<<bt->total[FAM_FZ], 256, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, +1);
+  k_fft_z<<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, +1, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
   PMARK(pf, AFID_K_FFT_Z_INV);
-  k_fft_y_inv<<<bt->total[FAM_FY], 256, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns);
+  k_fft_y_inv<<<bt->grid_y, FFT_T, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns, bt->sm_y, bt->total[FAM_FY]);
   CKL();
   PMARK(pf, AFID_K_FFT_Y_INV);
   return 0;
@@ -592,7 +623,8 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   if (!c || !p || !xc || !box_id) return fail(AFID_EINVAL, "box_add: null argument");
   if (p->nxm < 3 || p->nym < 2 || p->nzm < 2) return fail(AFID_EINVAL, "box_add: nxm >= 3, nym, nzm >= 2");
   if (p->nym % 2) return fail(AFID_EINVAL, "box_add: nym must be even (real FFT along y)");
-  if (p->nym > 8192 || p->nzm > 8192) return fail(AFID_ESIZE, "box_add: nym, nzm <= 8192");
+  if (p->nym > AFID_MAX_NYZ || p->nzm > AFID_MAX_NYZ)
+    return fail(AFID_ESIZE, "box_add: nym, nzm <= %d (one transform line per block)", AFID_MAX_NYZ);
   if (p->nsst != 1 && p->nsst != 3) return fail(AFID_EINVAL, "box_add: nsst must be 1 or 3");
   if (!(p->ray > 0) || !(p->pra > 0) || !(p->ylen > 0) || !(p->zlen > 0) || !(p->alx3 > 0))
     return fail(AFID_EINVAL, "box_add: ray, pra, ylen, zlen, alx3 must be > 0");
@@ -820,9 +852,9 @@ int afid_box_set_tuning(afid_ctx *c, int id, int fft_y_lines, int fft_z_lines, i
   int rc = get_box(c, id, &hb);
   if (rc) return rc;
   BoxDev &d = hb->dev;
-  if (fft_y_lines < 0 || fft_y_lines > fft_max_lines(d.nym, fft_nbuf(d.fft_y_np, false)))
+  if (fft_y_lines < 0 || (fft_y_lines > 0 && !fft_y_ok(d.nym, fft_y_lines, FFT_SMEM_MAX)))
     return fail(AFID_EINVAL, "fft_y_lines %d out of range", fft_y_lines);
-  if (fft_z_lines < 0 || fft_z_lines > fft_max_lines(d.nzm, fft_nbuf(d.fft_z_np, true)))
+  if (fft_z_lines < 0 || (fft_z_lines > 0 && !fft_z_ok(d.nzm, fft_z_lines, FFT_SMEM_MAX)))
     return fail(AFID_EINVAL, "fft_z_lines %d out of range", fft_z_lines);
   if (k1_minb != 0 && (k1_minb < 2 || k1_minb > 4)) return fail(AFID_EINVAL, "k1 variant must be 0, 2, 3 or 4");
   rc = set_device(c);
@@ -1096,7 +1128,7 @@ namespace {
 
 constexpr long long NOALLOC_MAX_SPEC = 1LL << 21;            // nxm * nzm * (nym/2 + 1)
 constexpr int NOALLOC_MAX_NXM = 1024;
-constexpr int NOALLOC_MAX_NYZ = 4096;
+constexpr int NOALLOC_MAX_NYZ = AFID_MAX_NYZ;
 constexpr long long NOALLOC_META = 1LL << 16;                // tables, twiddles, descriptors
 constexpr long long AFID_NOALLOC_DOUBLES = 3 * NOALLOC_MAX_SPEC + NOALLOC_META;
 
@@ -1232,17 +1264,23 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   const BoxDev *dbox = (const BoxDev *)(base + o_box);
   const int *doff = (const int *)(base + o_off);
   BatchDev fy{dbox, doff + 0, 1}, fz{dbox, doff + 2, 1}, px{dbox, doff + 4, 1};
-  const size_t sy = (size_t)fft_y_smem(d);
-  const size_t sz = (size_t)fft_z_smem(d);
-  k_fft_y_fwd<<<off[0][1], FFT_T, sy, st>>>(fy, 0);
+  FftSmem smy{0}, smz{0};
+  int twy = 0, twz = 0, gy = 0, gz = 0;
+  fft_smem_grow(d, smy, smz, twy, twz);
+  const size_t sy = (size_t)(2 * smy.slot + twy) * 16;
+  const size_t sz = (size_t)(2 * smz.slot + twz) * 16;
+  rc = fft_grid(k_fft_y_fwd, sy, off[0][1], &gy);
+  if (!rc) rc = fft_grid(k_fft_z, sz, off[1][1], &gz);
+  if (rc) return rc;
+  k_fft_y_fwd<<<gy, FFT_T, sy, st>>>(fy, 0, smy, off[0][1]);
   CKL();
-  k_fft_z<<<off[1][1], FFT_T, sz, st>>>(fz, 0, -1);
+  k_fft_z<<<gz, FFT_T, sz, st>>>(fz, 0, -1, smz, off[1][1]);
   CKL();
   k_poisson_x<<<off[2][1], 256, 0, st>>>(px, 0);
   CKL();
-  k_fft_z<<<off[1][1], FFT_T, sz, st>>>(fz, 0, +1);
+  k_fft_z<<<gz, FFT_T, sz, st>>>(fz, 0, +1, smz, off[1][1]);
   CKL();
-  k_fft_y_inv<<<off[0][1], FFT_T, sy, st>>>(fy, 0);
+  k_fft_y_inv<<<gy, FFT_T, sy, st>>>(fy, 0, smy, off[0][1]);
   CKL();
   return 0;
 }

@@ -138,4 +138,23 @@ __device__ __forceinline__ unsigned long long dbits(double v) {
   return (unsigned long long)__double_as_longlong(v);
 }
 
+// Asynchronous global -> shared copies (cp.async): 16 bytes bypassing L1,
+// 8 bytes through L1; groups are committed and waited for explicitly.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(src));
+}
+__device__ __forceinline__ void cp_async8d(void *dst, const void *src) {
+  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src));
+}
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) { cp_async8d(dst, src); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_commit_wait() {
+  cp_async_commit();
+  cp_async_wait_all();
+}
+
 }  // namespace afid

@@ -7,11 +7,11 @@
 // reads its lines directly from the plane-major layout.
 //
 // The FFTs are Stockham auto-sort passes of radix 16, 8, 4, 2, 3, 5 and 7
-// (plans in increasing radix order, e.g. 768 = 3 x 16 x 16): the first pass
-// streams from global memory, the inner passes run in place in shared memory
-// and the last pass of the z and inverse-y transforms streams back to global
-// memory.  Twiddles exp(-2 pi i n / N) come from a table computed on the host
-// in extended precision and copied to shared memory by every block.
+// (plans in increasing radix order, e.g. 768 = 3 x 16 x 16), run in place in
+// shared memory on tiles copied in with cp.async; the last pass of the z and
+// inverse-y transforms streams back to global memory.  Twiddles
+// exp(-2 pi i n / N) come from a table computed on the host in extended
+// precision and copied to shared memory by every block.
 #pragma once
 #include "afid_device.cuh"
 
@@ -136,18 +136,29 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
 // Stockham passes over L lines of length N.  Pass p with radix R reads
 // element j + r N/R of each butterfly j and writes element
 // (j / Ns) Ns R + j % Ns + r Ns, Ns being the product of the earlier radices.
-// Every pass streams from a source functor to a destination functor: the
-// first pass reads global memory, inner passes go between two shared
-// buffers, and the last pass of the z and inverse-y transforms writes global
-// memory.  LINE_MAJOR: element (l, n) at l*N + n, else at n*L + l.
-constexpr int FFT_T = 256;    // threads per FFT block
+// Passes run in place in one shared buffer: every thread first loads the
+// inputs of all its butterflies into registers, the block synchronises, and
+// the outputs are stored into the same buffer (then the block synchronises
+// again).  A thread takes at most 16 / R butterflies, i.e. holds at most 16
+// complex values, so a tile may hold at most FFT_TILE_MAX values.  The first
+// pass may read through a source functor (pairs of real rows, raw
+// half-spectrum rows) and the last pass may write through a destination
+// functor (global memory).  LINE_MAJOR: element (l, n) at l*N + n, else at
+// n*L + l.
+constexpr int FFT_T = 256;                  // threads per FFT block
+constexpr int FFT_TILE_MAX = 14 * FFT_T;    // complex values per tile (radix 7: 2 butterflies of 7)
 
-template <bool LM>
-__device__ __forceinline__ void bfly_index(int t, int NR, int L, int &l, int &j) {
-  if (LM) { j = t % NR; l = t / NR; } else { l = t % L; j = t / L; }
-}
-template <bool LM>
-__device__ __forceinline__ int sidx(int l, int n, int N, int L) { return LM ? l * N + n : n * L + l; }
+// Division by a positive int that is usually a power of two (lines per
+// tile always are; Ns is for plans with at most one odd radix).
+struct FastDiv {
+  int d, sh;
+  bool p2;
+  __device__ __forceinline__ explicit FastDiv(int d_) : d(d_), sh(0), p2((d_ & (d_ - 1)) == 0) {
+    while ((2 << sh) <= d) ++sh;
+  }
+  __device__ __forceinline__ int div(int n) const { return p2 ? (n >> sh) : n / d; }
+  __device__ __forceinline__ int mod(int n) const { return p2 ? (n & (d - 1)) : n % d; }
+};
 
 template <int R>
 __device__ __forceinline__ void twiddle(double2 (&v)[R], int k, int tstr, int sgn, const double2 *tw) {
@@ -159,199 +170,224 @@ __device__ __forceinline__ void twiddle(double2 (&v)[R], int k, int tstr, int sg
   }
 }
 
-template <int R, bool LM, class Src, class Dst>
-__device__ __forceinline__ void pass_stream(int N, int L, int Ns, int sgn, const double2 *tw,
-                                            const Src &src, const Dst &dst) {
-  const int NR = N / R, tstr = N / (Ns * R), total = NR * L;
-  for (int t = threadIdx.x; t < total; t += FFT_T) {
-    int l, j;
-    bfly_index<LM>(t, NR, L, l, j);
-    const int k = j % Ns;
-    double2 v[R];
+// element (l, n) of a tile of L lines (L a power of two) at n*L + l
+__device__ __forceinline__ int sidx(int l, int n, int lgL) { return (n << lgL) + l; }
+
+template <int R, class Src, class Dst>
+__device__ __forceinline__ void pass_inplace(int N, int lgL, int Ns, int sgn, const double2 *tw,
+                                             const Src &src, const Dst &dst) {
+  constexpr int BPT = 16 / R;               // butterflies per thread
+  const int NR = N / R, tstr = N / (Ns * R);
+  const int lmask = (1 << lgL) - 1;
+  const FastDiv dNs(Ns);
+  double2 v[BPT][R];
+  // every slot loads (idle ones repeat the last butterfly of their line): a
+  // conditional load here would keep v out of registers across the barrier
+  // thread t takes butterflies j = t / L + b FFT_T / L of line l = t % L
+  const int l = threadIdx.x & lmask, j0 = threadIdx.x >> lgL, jstep = FFT_T >> lgL;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src(l, j + r * NR);
-    if (Ns > 1) twiddle<R>(v, k, tstr, sgn, tw);
-    dft_small<R>(v, sgn, tw, N);
-    const int base = (j / Ns) * Ns * R + k;
+  for (int b = 0; b < BPT; ++b) {
+    const int jc = min(j0 + b * jstep, NR - 1);
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst(l, base + r * Ns, v[r]);
+    for (int r = 0; r < R; ++r) v[b][r] = src(l, jc + r * NR);
   }
-}
-
-template <bool LM, class Src, class Dst>
-__device__ __forceinline__ void run_stream(int R, int N, int L, int Ns, int sgn, const double2 *tw,
-                                           const Src &src, const Dst &dst) {
-  switch (R) {
-    case 16: pass_stream<16, LM>(N, L, Ns, sgn, tw, src, dst); break;
-    case 8: pass_stream<8, LM>(N, L, Ns, sgn, tw, src, dst); break;
-    case 4: pass_stream<4, LM>(N, L, Ns, sgn, tw, src, dst); break;
-    case 2: pass_stream<2, LM>(N, L, Ns, sgn, tw, src, dst); break;
-    case 3: pass_stream<3, LM>(N, L, Ns, sgn, tw, src, dst); break;
-    case 5: pass_stream<5, LM>(N, L, Ns, sgn, tw, src, dst); break;
-    default: pass_stream<7, LM>(N, L, Ns, sgn, tw, src, dst); break;
-  }
-}
-
-template <bool LM>
-struct SmemDst {
-  double2 *a; int N, L;
-  __device__ __forceinline__ void operator()(int l, int n, double2 v) const { a[sidx<LM>(l, n, N, L)] = v; }
-};
-template <bool LM>
-struct SmemSrc {
-  const double2 *a; int N, L;
-  __device__ __forceinline__ double2 operator()(int l, int n) const { return a[sidx<LM>(l, n, N, L)]; }
-};
-
-// Transform of L lines.  The first pass streams from ``src`` into shared
-// buffer a; inner passes ping-pong between a and b; the last pass streams to
-// ``dst`` when LAST_TO_DST, otherwise it lands in shared memory too.  Returns
-// the shared buffer holding the result (meaningful when !LAST_TO_DST).
-template <bool LM, bool LAST_TO_DST, class Src, class Dst>
-__device__ double2 *fft_lines(double2 *a, double2 *b, int N, int L, const int *rad, int np, int sgn,
-                              const double2 *tw, const Src &src, const Dst &dst) {
-  if (np == 1 && LAST_TO_DST) {
-    run_stream<LM>(rad[0], N, L, 1, sgn, tw, src, dst);
-    return a;
-  }
-  run_stream<LM>(rad[0], N, L, 1, sgn, tw, src, SmemDst<LM>{a, N, L});
   __syncthreads();
+#pragma unroll
+  for (int b = 0; b < BPT; ++b) {
+    const int j = j0 + b * jstep;
+    if (j < NR) {
+      const int k = dNs.mod(j);
+      if (Ns > 1) twiddle<R>(v[b], k, tstr, sgn, tw);
+      dft_small<R>(v[b], sgn, tw, N);
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst(l, base + r * Ns, v[b][r]);
+    }
+  }
+  __syncthreads();
+}
+
+template <class Src, class Dst>
+__device__ __forceinline__ void run_inplace(int R, int N, int lgL, int Ns, int sgn, const double2 *tw,
+                                            const Src &src, const Dst &dst) {
+  switch (R) {
+    case 16: pass_inplace<16>(N, lgL, Ns, sgn, tw, src, dst); break;
+    case 8: pass_inplace<8>(N, lgL, Ns, sgn, tw, src, dst); break;
+    case 4: pass_inplace<4>(N, lgL, Ns, sgn, tw, src, dst); break;
+    case 2: pass_inplace<2>(N, lgL, Ns, sgn, tw, src, dst); break;
+    case 3: pass_inplace<3>(N, lgL, Ns, sgn, tw, src, dst); break;
+    case 5: pass_inplace<5>(N, lgL, Ns, sgn, tw, src, dst); break;
+    default: pass_inplace<7>(N, lgL, Ns, sgn, tw, src, dst); break;
+  }
+}
+
+struct SmemDst {
+  double2 *a; int lgL;
+  __device__ __forceinline__ void operator()(int l, int n, double2 v) const { a[sidx(l, n, lgL)] = v; }
+};
+struct SmemSrc {
+  const double2 *a; int lgL;
+  __device__ __forceinline__ double2 operator()(int l, int n) const { return a[sidx(l, n, lgL)]; }
+};
+
+// Whole transform of a tile held in shared buffer a: the first pass reads
+// ``src``, the last pass writes ``dst`` when LAST_TO_DST (otherwise the
+// result stays in a).
+template <bool LAST_TO_DST, class Src, class Dst>
+__device__ void fft_tile(double2 *a, int N, int lgL, const int *rad, int np, int sgn, const double2 *tw,
+                         const Src &src, const Dst &dst) {
+  const SmemSrc as{a, lgL};
+  const SmemDst ad{a, lgL};
+  if (np == 1) {
+    if (LAST_TO_DST) run_inplace(rad[0], N, lgL, 1, sgn, tw, src, dst);
+    else run_inplace(rad[0], N, lgL, 1, sgn, tw, src, ad);
+    return;
+  }
+  run_inplace(rad[0], N, lgL, 1, sgn, tw, src, ad);
   int Ns = rad[0];
-  const int nin = LAST_TO_DST ? np - 1 : np;
-  for (int p = 1; p < nin; ++p) {
-    run_stream<LM>(rad[p], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, SmemDst<LM>{b, N, L});
-    __syncthreads();
-    double2 *t = a; a = b; b = t;
+  for (int p = 1; p < np - 1; ++p) {
+    run_inplace(rad[p], N, lgL, Ns, sgn, tw, as, ad);
     Ns *= rad[p];
   }
-  if (LAST_TO_DST) run_stream<LM>(rad[np - 1], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, dst);
-  return a;
+  if (LAST_TO_DST) run_inplace(rad[np - 1], N, lgL, Ns, sgn, tw, as, dst);
+  else run_inplace(rad[np - 1], N, lgL, Ns, sgn, tw, as, ad);
 }
 
-// Transform of L lines whose input is already in shared buffer a: every
-// pass goes shared -> shared (a, b alternating) except the last, which goes
-// to ``dst`` when LAST_TO_DST.  Returns the buffer holding the result
-// (meaningful when !LAST_TO_DST).
-template <bool LM, bool LAST_TO_DST, class Dst>
-__device__ double2 *fft_lines_smem(double2 *a, double2 *b, int N, int L, const int *rad, int np, int sgn,
-                                   const double2 *tw, const Dst &dst, int Ns0 = 1) {
-  int Ns = Ns0;
-  const int nin = LAST_TO_DST ? np - 1 : np;
-  for (int p = 0; p < nin; ++p) {
-    run_stream<LM>(rad[p], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, SmemDst<LM>{b, N, L});
-    __syncthreads();
-    double2 *t = a; a = b; b = t;
-    Ns *= rad[p];
-  }
-  if (LAST_TO_DST) run_stream<LM>(rad[np - 1], N, L, Ns, sgn, tw, SmemSrc<LM>{a, N, L}, dst);
-  return a;
-}
+// Persistent transform blocks.  A launch has at most (SMs x resident blocks)
+// blocks; each takes tiles blockIdx.x, blockIdx.x + gridDim.x, ... and
+// copies the next tile into its second shared-memory slot (cp.async) while
+// it transforms the current one in place.  Shared memory: two slots and the
+// twiddles of the box being transformed.  Lines per tile default to what
+// keeps two blocks on an SM (and at most FFT_TILE_MAX values per tile); the
+// tuning fields may choose other values within those limits.
+constexpr int FFT_SMEM_DEFAULT = 110 * 1024;
+constexpr int FFT_SMEM_MAX = 200 * 1024;
+constexpr int FFT_MAX_LINES = 16;
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(src));
+// y: a slot holds the 2 Pp real rows of a forward tile (Pp N complex) or the
+// 2 Pp half-spectrum rows of an inverse tile (2 Pp (N/2+1) complex)
+__host__ __device__ __forceinline__ int fft_y_slot(int N, int Pp) { return 2 * Pp * (N / 2 + 1); }  // >= Pp (N + 1)
+__host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 * fft_y_slot(N, Pp) + N) * 16; }
+__host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16; }
+__host__ __device__ __forceinline__ bool fft_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
+__host__ __device__ __forceinline__ bool fft_y_ok(int N, int Pp, int budget) {
+  return fft_pow2(Pp) && Pp * N <= FFT_TILE_MAX && fft_y_bytes(N, Pp) <= budget;
 }
-__device__ __forceinline__ void cp_async8d(void *dst, const void *src) {
-  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src));
+__host__ __device__ __forceinline__ bool fft_z_ok(int N, int L, int budget) {
+  return fft_pow2(L) && L * N <= FFT_TILE_MAX && fft_z_bytes(N, L) <= budget;
 }
-__device__ __forceinline__ void cp_async_commit_wait() {
-  asm volatile("cp.async.commit_group;\n" ::);
-  asm volatile("cp.async.wait_all;\n" ::);
+__host__ __device__ __forceinline__ int fft_fit_lines(int N, int budget, bool y) {
+  int l = FFT_MAX_LINES;
+  while (l > 1 && !(y ? fft_y_ok(N, l, budget) : fft_z_ok(N, l, budget))) l >>= 1;
+  return l;
 }
-
-// Lines per block and shared memory: two (lines x N) buffers when the
-// transform has a pass between two shared-memory stages, otherwise one, plus
-// the N twiddles; lines are capped so that a block stays within ~100 KB.
-__host__ __device__ __forceinline__ int fft_nbuf(int np, bool last_to_dst) {
-  // the copied-in tile plus one buffer per pass that writes shared memory,
-  // ping-ponging: two buffers unless the only pass streams straight out
-  const int smem_stages = last_to_dst ? np - 1 : np;
-  return smem_stages >= 1 ? 2 : 1;
-}
-__host__ __device__ __forceinline__ int fft_lines_per_block(int N, int nbuf, int cap) {
-  int l = (100 * 1024) / (16 * N * nbuf);
-  if (l > cap) l = cap;
-  return l < 1 ? 1 : l;
+__host__ __device__ __forceinline__ int ilog2(int v) {
+  int r = 0;
+  while ((1 << (r + 1)) <= v) ++r;
+  return r;
 }
 __host__ __device__ __forceinline__ int fft_y_pairs(const BoxDev &B) {
   if (B.fy_lines > 0) return B.fy_lines;
-  return fft_lines_per_block(B.nym, fft_nbuf(B.fft_y_np, false), 16);
+  return fft_fit_lines(B.nym, FFT_SMEM_DEFAULT, true);
 }
 __host__ __device__ __forceinline__ int fft_z_lines(const BoxDev &B) {
-  const int l = B.fz_lines > 0 ? B.fz_lines : fft_lines_per_block(B.nzm, fft_nbuf(B.fft_z_np, true), 16);
-  return l < B.nymh ? l : B.nymh;
+  int l = B.fz_lines > 0 ? B.fz_lines : fft_fit_lines(B.nzm, FFT_SMEM_DEFAULT, false);
+  while (l > 1 && l / 2 >= B.nymh) l >>= 1;   // no tile wider than needed
+  return l;
 }
-// largest admissible tuning values (shared memory of one block <= 200 KB)
-__host__ __device__ __forceinline__ int fft_max_lines(int N, int nbuf) {
-  return (200 * 1024) / (16 * N * nbuf) - 1;
-}
-__host__ __device__ __forceinline__ int fft_y_smem(const BoxDev &B) {
-  // forward: lines + copied-in rows + twiddles; inverse: lines + raw
-  // half-spectrum rows (2 Pp (nym/2+1) complex) + twiddles
-  const int Pp = fft_y_pairs(B);
-  return ((2 * Pp + 1) * B.nym + 2 * Pp) * 16;
-}
-__host__ __device__ __forceinline__ int fft_z_smem(const BoxDev &B) {
-  return (fft_nbuf(B.fft_z_np, true) * fft_z_lines(B) + 1) * B.nzm * 16;
+
+// shared-memory layout of one launch (largest box of the batch)
+struct FftSmem {
+  int slot;   // complex values per copy-in slot (the twiddles follow the two slots)
+};
+
+__device__ __forceinline__ int tile_box(const BatchDev &bt, int tile, int &local) {
+  const int b = find_box(bt.tile_off, bt.nbox, tile);
+  local = tile - __ldg(bt.tile_off + b);
+  return b;
 }
 
 // ---------------------------------------------------------------------------
 // y forward: rows (k, i) of length nym of dph -> spec[k][i][ky], ky <= nym/2.
+// A tile is 2 Pp consecutive rows of one plane; line p of the transform is
+// the complex pair (row 2p, row 2p+1), unpacked after the last pass into the
+// two half spectra.
 // ---------------------------------------------------------------------------
 struct NoDst {
   __device__ __forceinline__ void operator()(int, int, double2) const {}
 };
+// rows are copied in with a stride of nym + 1 doubles, which spreads the
+// rows of one column over the shared-memory banks
+struct PairSrc {
+  const double *rows; int RS;
+  __device__ __forceinline__ double2 operator()(int p, int n) const {
+    return make_double2(rows[2 * p * RS + n], rows[(2 * p + 1) * RS + n]);
+  }
+};
 
-// y forward over the rows of dph (phi): the 2*Pp rows of the block are
-// copied into shared memory with cp.async, packed two by two as complex
-// lines, transformed, and unpacked into the half spectrum.
-__global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
-  extern __shared__ double2 fsm[];
-  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
-  const BoxDev &B = bt.boxes[b];
-  if (!B.active || ns >= B.nsst) return;
-  const BoxScalars *S = B.sc;
-  if (S->status != 0) return;
-  const int N = B.nym, nzm = B.nzm;
-  const int Pp = fft_y_pairs(B);
+__device__ __forceinline__ void fft_y_fwd_copy_in(const BoxDev &B, int lt, double *rows) {
+  const int N = B.nym, nzm = B.nzm, Pp = fft_y_pairs(B);
   const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
-  const int tile = blockIdx.x - __ldg(bt.tile_off + b);
-  const int k = tile / groups;
-  const int i0 = (tile - k * groups) * 2 * Pp;
-  double2 *a = fsm, *bb = fsm + Pp * N, *tws = fsm + 2 * Pp * N;
-  // copy in: row r of the block (i = i0 + r) as doubles into bb; line p is
-  // the complex pair (row 2p, row 2p+1), re-read below as double2 from a
-  double *rows = (double *)bb;
+  const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
   const double *phik = B.phi + (long long)k * B.plane;
   for (int t = threadIdx.x; t < 2 * Pp * N; t += FFT_T) {
     const int r = t / N, j = t - r * N;
-    if (i0 + r < nzm) cp_async8d(rows + r * N + j, phik + (long long)(i0 + r) * N + j);
-    else rows[r * N + j] = 0.0;
+    if (i0 + r < nzm) cp_async8d(rows + r * (N + 1) + j, phik + (long long)(i0 + r) * N + j);
+    else rows[r * (N + 1) + j] = 0.0;
   }
-  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twy + t);
-  cp_async_commit_wait();
-  __syncthreads();
-  for (int t = threadIdx.x; t < Pp * N; t += FFT_T) {
-    const int p = t / N, j = t - p * N;
-    a[p * N + j] = make_double2(rows[2 * p * N + j], rows[(2 * p + 1) * N + j]);
+}
+
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, FftSmem sm, int total) {
+  extern __shared__ double2 fsm[];
+  double2 *slot[2] = {fsm, fsm + sm.slot};
+  double2 *tws = fsm + 2 * sm.slot;
+  int t = blockIdx.x, loaded = -1, lt;
+  if (t < total) {
+    const int b = tile_box(bt, t, lt);
+    fft_y_fwd_copy_in(bt.boxes[b], lt, (double *)slot[0]);
   }
-  __syncthreads();
-  a = fft_lines_smem<true, false>(a, bb, N, Pp, B.fft_y_radix, B.fft_y_np, -1, tws, NoDst{});
-  // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
-  // B = (Z_q - conj Z_{N-q}) / (2i)
-  const int nh = B.nymh;
-  for (int t = threadIdx.x; t < Pp * nh; t += FFT_T) {
-    const int p = t / nh, q = t - p * nh;
-    const int i = i0 + 2 * p;
-    if (i >= nzm) continue;
-    const double2 z = a[p * N + q];
-    const double2 zn = a[p * N + (q == 0 ? 0 : N - q)];
-    const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
-    const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
-    const long long base = ((long long)k * nzm + i) * nh + q;
-    B.spec[base] = A;
-    if (i + 1 < nzm) B.spec[base + nh] = Bv;
+  cp_async_commit();
+  for (int it = 0; t < total; ++it, t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tn < total) {
+      int ln;
+      const int bn = tile_box(bt, tn, ln);
+      fft_y_fwd_copy_in(bt.boxes[bn], ln, (double *)slot[(it + 1) & 1]);
+    }
+    cp_async_commit();
+    cp_async_wait_1();
+    const int b = tile_box(bt, t, lt);
+    const BoxDev &B = bt.boxes[b];
+    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
+    if (run && b != loaded) {
+      for (int q = threadIdx.x; q < B.nym; q += FFT_T) tws[q] = __ldg(B.twy + q);
+      loaded = b;
+    }
+    __syncthreads();
+    if (run) {
+      const int N = B.nym, nzm = B.nzm, Pp = fft_y_pairs(B), nh = B.nymh;
+      const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
+      const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
+      double2 *cur = slot[it & 1];
+      const int lgP = ilog2(Pp);
+      fft_tile<false>(cur, N, lgP, B.fft_y_radix, B.fft_y_np, -1, tws, PairSrc{(const double *)cur, N + 1},
+                      NoDst{});
+      // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
+      // B = (Z_q - conj Z_{N-q}) / (2i)
+      for (int u = threadIdx.x; u < Pp * nh; u += FFT_T) {
+        const int p = u & (Pp - 1), q = u >> lgP;
+        const int i = i0 + 2 * p;
+        if (i >= nzm) continue;
+        const double2 z = cur[sidx(p, q, lgP)];
+        const double2 zn = cur[sidx(p, q == 0 ? 0 : N - q, lgP)];
+        const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
+        const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
+        const long long base = ((long long)k * nzm + i) * nh + q;
+        B.spec[base] = A;
+        if (i + 1 < nzm) B.spec[base + nh] = Bv;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -359,13 +395,6 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns) {
 // z transform in place on spec[k][kz][ky] for a tile of L consecutive ky.
 // Forward transforms divide by nym*nzm (SolvePressureCorrection.F90:105).
 // ---------------------------------------------------------------------------
-struct ZSrc {
-  const double2 *spec; int nh, ky0;
-  __device__ __forceinline__ double2 operator()(int l, int n) const {
-    const int ky = ky0 + l;
-    return ky < nh ? spec[(long long)n * nh + ky] : make_double2(0.0, 0.0);
-  }
-};
 struct ZDst {
   double2 *spec; int nh, ky0; double norm; bool scale;
   __device__ __forceinline__ void operator()(int l, int n, double2 v) const {
@@ -376,31 +405,56 @@ struct ZDst {
   }
 };
 
-__global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn) {
-  extern __shared__ double2 fsm[];
-  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
-  const BoxDev &B = bt.boxes[b];
-  if (!B.active || ns >= B.nsst) return;
-  if (B.sc->status != 0) return;
-  const int N = B.nzm, nh = B.nymh;
-  const int L = fft_z_lines(B);
+__device__ __forceinline__ void fft_z_copy_in(const BoxDev &B, int lt, double2 *a) {
+  const int N = B.nzm, nh = B.nymh, L = fft_z_lines(B);
   const int ntl = (nh + L - 1) / L;
-  const int tile = blockIdx.x - __ldg(bt.tile_off + b);
-  const int k = tile / ntl;
-  const int ky0 = (tile - k * ntl) * L;
-  const int nb = fft_nbuf(B.fft_z_np, true);
-  double2 *a = fsm, *bb = fsm + (nb - 1) * L * N, *tws = fsm + nb * L * N;
-  double2 *spec = B.spec + (long long)k * N * nh;
+  const int k = lt / ntl, ky0 = (lt - k * ntl) * L;
+  const double2 *spec = B.spec + (long long)k * N * nh;
   for (int t = threadIdx.x; t < L * N; t += FFT_T) {
     const int l = t % L, n = t / L;
-    if (ky0 + l < nh) cp_async16(a + n * L + l, spec + (long long)n * nh + ky0 + l);
-    else a[n * L + l] = make_double2(0.0, 0.0);
+    if (ky0 + l < nh) cp_async16(a + t, spec + (long long)n * nh + ky0 + l);
+    else a[t] = make_double2(0.0, 0.0);
   }
-  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twz + t);
-  cp_async_commit_wait();
-  __syncthreads();
-  fft_lines_smem<false, true>(a, bb, N, L, B.fft_z_radix, B.fft_z_np, sgn, tws,
-                              ZDst{spec, nh, ky0, (double)(B.nzm * B.nym), sgn < 0});
+}
+
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn, FftSmem sm, int total) {
+  extern __shared__ double2 fsm[];
+  double2 *slot[2] = {fsm, fsm + sm.slot};
+  double2 *tws = fsm + 2 * sm.slot;
+  int t = blockIdx.x, loaded = -1, lt;
+  if (t < total) {
+    const int b = tile_box(bt, t, lt);
+    fft_z_copy_in(bt.boxes[b], lt, slot[0]);
+  }
+  cp_async_commit();
+  for (int it = 0; t < total; ++it, t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tn < total) {
+      int ln;
+      const int bn = tile_box(bt, tn, ln);
+      fft_z_copy_in(bt.boxes[bn], ln, slot[(it + 1) & 1]);
+    }
+    cp_async_commit();
+    cp_async_wait_1();
+    const int b = tile_box(bt, t, lt);
+    const BoxDev &B = bt.boxes[b];
+    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
+    if (run && b != loaded) {
+      for (int q = threadIdx.x; q < B.nzm; q += FFT_T) tws[q] = __ldg(B.twz + q);
+      loaded = b;
+    }
+    __syncthreads();
+    if (run) {
+      const int N = B.nzm, nh = B.nymh, L = fft_z_lines(B);
+      const int ntl = (nh + L - 1) / L;
+      const int k = lt / ntl, ky0 = (lt - k * ntl) * L;
+      double2 *cur = slot[it & 1];
+      const int lgL = ilog2(L);
+      fft_tile<true>(cur, N, lgL, B.fft_z_radix, B.fft_z_np, sgn, tws, SmemSrc{cur, lgL},
+                            ZDst{B.spec + (long long)k * N * nh, nh, ky0, (double)(B.nzm * B.nym), sgn < 0});
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -517,43 +571,58 @@ struct YInvDst {
 
 // y inverse (complex-to-real, unnormalised): spec[k][i][ky] -> phi[k][i][j].
 // As in a c2r transform, the imaginary parts of the ky = 0 and ky = nym/2
-// coefficients are ignored.  The block's half-spectrum rows are copied into
-// shared memory with cp.async; two rows are recovered from one complex line
-// Z = A + i B.  The raw rows' buffer becomes the second ping-pong buffer once
-// the first pass has read it.
-__global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns) {
-  extern __shared__ double2 fsm[];
-  const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
-  const BoxDev &B = bt.boxes[b];
-  if (!B.active || ns >= B.nsst) return;
-  if (B.sc->status != 0) return;
-  const int N = B.nym, nzm = B.nzm, nh = B.nymh;
-  const int Pp = fft_y_pairs(B);
+// coefficients are ignored.  A tile's 2 Pp half-spectrum rows are copied
+// into a slot; two rows are recovered from one complex line Z = A + i B,
+// which the first pass writes over the raw rows it has read.
+__device__ __forceinline__ void fft_y_inv_copy_in(const BoxDev &B, int lt, double2 *raw) {
+  const int nzm = B.nzm, nh = B.nymh, Pp = fft_y_pairs(B);
   const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
-  const int tile = blockIdx.x - __ldg(bt.tile_off + b);
-  const int k = tile / groups;
-  const int i0 = (tile - k * groups) * 2 * Pp;
-  // layout: a = Pp*N, raw (= b) = 2*Pp*nh >= Pp*N, twiddles
-  double2 *a = fsm, *raw = fsm + Pp * N, *tws = raw + 2 * Pp * nh;
+  const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
   const double2 *speck = B.spec + (long long)k * nzm * nh;
   for (int t = threadIdx.x; t < 2 * Pp * nh; t += FFT_T) {
     const int r = t / nh, q = t - r * nh;
     if (i0 + r < nzm) cp_async16(raw + t, speck + (long long)(i0 + r) * nh + q);
     else raw[t] = make_double2(0.0, 0.0);
   }
-  for (int t = threadIdx.x; t < N; t += FFT_T) tws[t] = __ldg(B.twy + t);
-  cp_async_commit_wait();
-  __syncthreads();
-  const int np = B.fft_y_np;
-  YInvDst dst{B.phi + (long long)k * B.plane, N, nzm, i0};
-  const YInvSmemSrc src{raw, N, nh, (N % 2) == 0};
-  if (np == 1) {
-    run_stream<true>(B.fft_y_radix[0], N, Pp, 1, +1, tws, src, dst);
-    return;
+}
+
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, FftSmem sm, int total) {
+  extern __shared__ double2 fsm[];
+  double2 *slot[2] = {fsm, fsm + sm.slot};
+  double2 *tws = fsm + 2 * sm.slot;
+  int t = blockIdx.x, loaded = -1, lt;
+  if (t < total) {
+    const int b = tile_box(bt, t, lt);
+    fft_y_inv_copy_in(bt.boxes[b], lt, slot[0]);
   }
-  run_stream<true>(B.fft_y_radix[0], N, Pp, 1, +1, tws, src, SmemDst<true>{a, N, Pp});
-  __syncthreads();
-  fft_lines_smem<true, true>(a, raw, N, Pp, B.fft_y_radix + 1, np - 1, +1, tws, dst, B.fft_y_radix[0]);
+  cp_async_commit();
+  for (int it = 0; t < total; ++it, t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tn < total) {
+      int ln;
+      const int bn = tile_box(bt, tn, ln);
+      fft_y_inv_copy_in(bt.boxes[bn], ln, slot[(it + 1) & 1]);
+    }
+    cp_async_commit();
+    cp_async_wait_1();
+    const int b = tile_box(bt, t, lt);
+    const BoxDev &B = bt.boxes[b];
+    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
+    if (run && b != loaded) {
+      for (int q = threadIdx.x; q < B.nym; q += FFT_T) tws[q] = __ldg(B.twy + q);
+      loaded = b;
+    }
+    __syncthreads();
+    if (run) {
+      const int N = B.nym, nzm = B.nzm, nh = B.nymh, Pp = fft_y_pairs(B);
+      const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
+      const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
+      double2 *cur = slot[it & 1];
+      fft_tile<true>(cur, N, ilog2(Pp), B.fft_y_radix, B.fft_y_np, +1, tws, YInvSmemSrc{cur, N, nh, (N % 2) == 0},
+                           YInvDst{B.phi + (long long)k * B.plane, N, nzm, i0});
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace afid

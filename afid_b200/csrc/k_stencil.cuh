@@ -266,13 +266,6 @@ struct RingAcc {
   }
 };
 
-__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
-  unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int k) {
   switch (t) {
@@ -303,7 +296,10 @@ __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int 
 // load has two barrier intervals of compute to arrive in.  Plane k-1 is not
 // read from the ring: the seven values of it that the stencils need are kept
 // in registers.  The RK history of the next PPB planes is loaded into
-// registers one interval ahead.  Writes the RK history (rux.. = H) and the
+// registers one interval ahead.  Global loads and stores use the global
+// state space explicitly (ld.global / st.global intrinsics), so the compiler
+// knows they cannot touch the shared ring and keeps stencil values in
+// registers across them.  Writes the RK history (rux.. = H) and the
 // forward-sweep values y of each solve; the temperature sweep starts from
 // y(1) = 0 and the missing contribution of its wall row is added by K2 (the
 // solve is linear in y(1)).
@@ -378,7 +374,7 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
   auto load_hist = [&](int p, double (&h)[4]) {
     if (inside && p <= nxm - 1) {
       const long long o = (long long)p * P + col;
-      h[0] = B.rux[o]; h[1] = B.ruy[o]; h[2] = B.ruz[o]; h[3] = B.rutemp[o];
+      h[0] = __ldcg(B.rux + o); h[1] = __ldcg(B.ruy + o); h[2] = __ldcg(B.ruz + o); h[3] = __ldcg(B.rutemp + o);
     }
   };
 
@@ -430,20 +426,20 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
           const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
           const double r = rhs_vyz(H, hc[u][1], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
                                    acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
-          B.ruy[o] = H;
+          __stwb(B.ruy + o, H);
           const double bb = r * tk[KT_YSC];
           yY = (kc == 0) ? bb : bb - tk[KT_YF] * yY;
-          B.ybuf[1][o] = yY;
+          __stwb(B.ybuf[1] + o, yY);
         }
         {
           const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
           const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
           const double r = rhs_vyz(H, hc[u][2], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
                                    acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
-          B.ruz[o] = H;
+          __stwb(B.ruz + o, H);
           const double bb = r * tk[KT_YSC];
           yZ = (kc == 0) ? bb : bb - tk[KT_YF] * yZ;
-          B.ybuf[2][o] = yZ;
+          __stwb(B.ybuf[2] + o, yZ);
         }
         if (kc >= 1) {
           const double udx3c_k = tk[KT_UDX3C];
@@ -453,19 +449,19 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
             const double r = rhs_vx(H, hc[u][0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
                                     acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
                                     am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
-            B.rux[o] = H;
+            __stwb(B.rux + o, H);
             const double bb = r * tk[KT_XSC];
             yX = bb - tk[KT_XF] * yX;
-            B.ybuf[0][o] = yX;
+            __stwb(B.ybuf[0] + o, yX);
           }
           {
             const double H = h_temp(acc, c, udx3c_k);
             const double r = rhs_temp(H, hc[u][3], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
                                       acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
-            B.rutemp[o] = H;
+            __stwb(B.rutemp + o, H);
             const double bb = r * tk[KT_TSC];
             yT = bb - tk[KT_TF] * yT;
-            B.ybuf[3][o] = yT;
+            __stwb(B.ybuf[3] + o, yT);
           }
         }
         // stash what plane kc+1 will need of this plane
@@ -731,43 +727,64 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-__global__ void __launch_bounds__(256) k_diag(BatchDev bt) {
+// Column march as in k_divergence: one thread per (j, i); vx(k+1) of one
+// plane is vx(k) of the next, so every field is read once.
+__global__ void __launch_bounds__(256, 2) k_diag(BatchDev bt) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active) return;
   BoxScalars *S = B.sc;
   if (S->status != 0) return;
   const long long P = B.plane;
-  const long long n = (long long)B.nxm * P;
-  const long long base = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x * 4;
-  double cfl = 0.0, dv = 0.0, vy = 0.0, vz = 0.0;
+  const long long col = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
+  double cfl = 0.0, dv = 0.0, my = 0.0, mz = 0.0;
   int bad = 0;
-  for (int r = 0; r < 4; ++r) {
-    const long long cell = base + r * blockDim.x + threadIdx.x;
-    if (cell >= n) break;
-    const int k = (int)(cell / P);
-    const long long col = cell - (long long)k * P;
-    const int i = (int)(col / B.nym);
-    const int j = (int)(col - (long long)i * B.nym);
-    const int ip = i == B.nzm - 1 ? 0 : i + 1;
-    const int jp = j == B.nym - 1 ? 0 : j + 1;
-    const double udx3m = tabk(B, T_UDX3M, k);
-    const double vzc = B.vz[cell], vzp = B.vz[(long long)k * P + (long long)ip * B.nym + j];
-    const double vyc = B.vy[cell], vyp = B.vy[(long long)k * P + (long long)i * B.nym + jp];
-    const double vxc = B.vx[cell], vxp = B.vx[cell + P];
-    const double q = fabs((vzc + vzp) * 0.5 * B.dz) + fabs((vyc + vyp) * 0.5 * B.dy)
-                   + fabs((vxc + vxp) * 0.5 * udx3m);
-    const double d = (vzp - vzc) * B.dz + (vyp - vyc) * B.dy + (vxp - vxc) * udx3m;
-    if (!isfinite(q) || !isfinite(d) || !isfinite(B.temp[cell])) bad = 1;
-    cfl = fmax(cfl, q);
-    dv = fmax(dv, fabs(d));
-    vy = fmax(vy, fabs(vyc));
-    vz = fmax(vz, fabs(vzc));
+  if (col < P) {
+    const int nym = B.nym, nzm = B.nzm, nxm = B.nxm;
+    const int i = (int)(col / nym);
+    const int j = (int)(col - (long long)i * nym);
+    const long long oip = (long long)(i == nzm - 1 ? 0 : i + 1) * nym + j - col;
+    const long long ojp = (long long)i * nym + (j == nym - 1 ? 0 : j + 1) - col;
+    const double *__restrict__ vx = B.vx + col;
+    const double *__restrict__ vy = B.vy + col;
+    const double *__restrict__ vz = B.vz + col;
+    const double *__restrict__ tp = B.temp + col;
+    const double dz = B.dz, dy = B.dy;
+    double xk = vx[0];
+    for (int k0 = 0; k0 < nxm; k0 += KD_U) {
+      double zc[KD_U], zp[KD_U], yc[KD_U], yp[KD_U], xn[KD_U], tc[KD_U];
+#pragma unroll
+      for (int u = 0; u < KD_U; ++u) {
+        const int k = k0 + u;
+        if (k < nxm) {
+          const long long o = (long long)k * P;
+          zc[u] = vz[o]; zp[u] = vz[o + oip];
+          yc[u] = vy[o]; yp[u] = vy[o + ojp];
+          xn[u] = vx[o + P];
+          tc[u] = tp[o];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < KD_U; ++u) {
+        const int k = k0 + u;
+        if (k >= nxm) break;
+        const double udx3m = tabk(B, T_UDX3M, k);
+        const double q = fabs((zc[u] + zp[u]) * 0.5 * dz) + fabs((yc[u] + yp[u]) * 0.5 * dy)
+                       + fabs((xk + xn[u]) * 0.5 * udx3m);
+        const double d = (zp[u] - zc[u]) * dz + (yp[u] - yc[u]) * dy + (xn[u] - xk) * udx3m;
+        if (!isfinite(q) || !isfinite(d) || !isfinite(tc[u])) bad = 1;
+        cfl = fmax(cfl, q);
+        dv = fmax(dv, fabs(d));
+        my = fmax(my, fabs(yc[u]));
+        mz = fmax(mz, fabs(zc[u]));
+        xk = xn[u];
+      }
+    }
   }
-  cfl = warp_max(cfl); dv = warp_max(dv); vy = warp_max(vy); vz = warp_max(vz);
+  cfl = warp_max(cfl); dv = warp_max(dv); my = warp_max(my); mz = warp_max(mz);
   __shared__ double sm[4][8];
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) { sm[0][w] = cfl; sm[1][w] = dv; sm[2][w] = vy; sm[3][w] = vz; }
+  if (l == 0) { sm[0][w] = cfl; sm[1][w] = dv; sm[2][w] = my; sm[3][w] = mz; }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&S->nonfinite, 1);
   if (threadIdx.x < 4) {
     double m = 0.0;

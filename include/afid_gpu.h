@@ -43,6 +43,10 @@ extern "C" {
 #define AFID_EFFT (-5)      /* nym or nzm has a prime factor > 7 (main.F90:156-165, code 444) */
 #define AFID_ESIZE (-6)     /* size beyond a fixed limit of the entry point */
 
+/* Largest nym and nzm of a box: one line of either transform, with its
+ * twiddles, must fit a block's shared memory. */
+#define AFID_MAX_NYZ 3072
+
 typedef struct afid_ctx afid_ctx;
 
 /* Fields a box holds (the arrays of module local_arrays, param.F90:80-87). */
@@ -112,7 +116,7 @@ size_t afid_box_device_bytes(const afid_box_params *p);
 /* Create a box: allocates its fields (zeroed, as AllocateReal3DArray does,
  * AuxiliaryRoutines.F90:79-97) and computes its metrics (CreateGrid.F90,
  * InitPressureSolver.F90) and time-scheme constants
- * (InitTimeMarchScheme.F90). */
+ * (InitTimeMarchScheme.F90).  nym, nzm <= AFID_MAX_NYZ. */
 int afid_box_add(afid_ctx *ctx, const afid_box_params *p, const double *xc, int *box_id);
 int afid_box_remove(afid_ctx *ctx, int box_id);
 int afid_box_upload(afid_ctx *ctx, int box_id, int field, const double *host);
@@ -198,7 +202,7 @@ int afid_step_profiled(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps,
  *          device layout dph[k][i][j] (y fastest, then z, then x)
  *   xc     host pointer: the nx = nxm+1 node positions
  *   stream cudaStream_t to queue the work on (0: the default stream)
- * Limits: nxm <= 1024, nym and nzm <= 4096 (nym even, prime factors <= 7),
+ * Limits: nxm <= 1024, nym and nzm <= 3072 (nym even, prime factors <= 7),
  * nxm*nzm*(nym/2+1) <= 2^21; larger boxes return AFID_ESIZE.
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture.  All calls share the array and find

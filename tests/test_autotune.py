@@ -5,9 +5,9 @@ from afid_b200 import BouIn
 from afid_b200.autotune import candidates, fft_plan, TuneCache
 
 
-@pytest.mark.parametrize("n,plan", [(768, [3, 16, 16]), (1280, [5, 16, 16]), (384, [3, 8, 16]),
-                                    (96, [2, 3, 16]), (48, [3, 16]), (32, [2, 16]), (64, [4, 16]),
-                                    (128, [8, 16]), (16, [16]), (12, [3, 4]), (14, [2, 7])])
+@pytest.mark.parametrize("n,plan", [(768, [16, 16, 3]), (1280, [16, 16, 5]), (384, [16, 8, 3]),
+                                    (96, [16, 2, 3]), (48, [16, 3]), (32, [16, 2]), (64, [16, 4]),
+                                    (128, [16, 8]), (16, [16]), (12, [4, 3]), (14, [2, 7])])
 def test_fft_plan(n, plan):
     assert fft_plan(n) == plan
     prod = 1
@@ -25,9 +25,12 @@ def test_fft_plan_rejects_large_primes():
 def test_candidates_fit_shared_memory(nyz):
     c = candidates(BouIn(nxm=64, nym=nyz, nzm=nyz))
     for v in c["fft_y_lines"]:
-        assert (2 * v + 1) * nyz * 16 <= 200 * 1024
+        assert (4 * v * (nyz // 2 + 1) + nyz) * 16 <= 200 * 1024 and v * nyz <= 14 * 256
+        assert v & (v - 1) == 0
     for v in c["fft_z_lines"]:
-        assert (2 * v + 1) * nyz * 16 <= 200 * 1024 and v <= nyz // 2 + 1
+        assert (2 * v * nyz + nyz) * 16 <= 200 * 1024 and v * nyz <= 14 * 256
+        assert v & (v - 1) == 0
+    assert c["fft_y_lines"] and c["fft_z_lines"]
     assert c["k1_minb"] == [2, 3, 4]
 
 
