@@ -69,7 +69,7 @@ struct Batch {
   int grid_y = 0, grid_z = 0;       // their resident grids
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
-  int k1_minb = 2;          // variant of the explicit/forward kernel (tuning, 2..4)
+  int k1_minb = 2;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
 };
 
 long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
@@ -94,9 +94,17 @@ int factor_radices(int n, int *rad, int *np) {
   return 0;
 }
 
-long long tiles_of(const BoxDev &B, int fam) {
+// Variants of the explicit/forward kernel: tile height TI (block of 32 TI
+// threads), resident blocks per SM and planes per barrier.
+//   2: 32x8 tiles, 2 blocks/SM        3: 32x8 tiles, 3 blocks/SM (80 registers)
+//   4: 32x8 tiles, two planes per barrier
+//   5: 32x4 tiles, 4 blocks/SM        6: 32x2 tiles, 8 blocks/SM
+constexpr int K1_VMIN = 2, K1_VMAX = 6;
+int k1_tile_height(int variant) { return variant == 5 ? 4 : variant == 6 ? 2 : 8; }
+
+long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2) {
   switch (fam) {
-    case FAM_K1: return cdiv(B.nym, K1_TJ) * cdiv(B.nzm, K1_TI);
+    case FAM_K1: return cdiv(B.nym, K1_TJ) * cdiv(B.nzm, k1_tile_height(k1_variant));
     case FAM_COL: return cdiv(B.plane, 256);
     case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
     case FAM_DIAG: return cdiv(B.plane, 256);
@@ -308,11 +316,22 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   }
   bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16;
   bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16;
+  {
+    // one variant of the explicit/forward kernel per launch: the one the
+    // boxes holding most of the cells ask for
+    long long w[K1_VMAX + 1] = {};
+    for (const BoxDev &d : devs) w[d.k1_minb >= K1_VMIN && d.k1_minb <= K1_VMAX ? d.k1_minb : 2] += d.fsize;
+    bt->k1_minb = 2;
+    for (int v = K1_VMIN; v <= K1_VMAX; ++v)
+      if (w[v] > w[bt->k1_minb]) bt->k1_minb = v;
+    const char *e = getenv("AFID_K1_VARIANT");
+    if (e && atoi(e) >= K1_VMIN && atoi(e) <= K1_VMAX) bt->k1_minb = atoi(e);
+  }
   for (int f = 0; f < NFAM; ++f) {
     long long acc = 0;
     for (int b = 0; b < n; ++b) {
       off[(size_t)f * (n + 1) + b] = (int)acc;
-      acc += tiles_of(devs[b], f);
+      acc += tiles_of(devs[b], f, bt->k1_minb);
     }
     if (acc > 0x7fffffffLL) { delete bt; return fail(AFID_ESIZE, "grid too large"); }
     off[(size_t)f * (n + 1) + n] = (int)acc;
@@ -331,15 +350,6 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     if (!rc) rc = fft_grid(k_fft_z, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
     if (rc) { free_batch(bt); return rc; }
   }
-  {
-    long long w[5] = {0, 0, 0, 0, 0};
-    for (const BoxDev &d : devs) w[d.k1_minb >= 2 && d.k1_minb <= 4 ? d.k1_minb : 2] += d.fsize;
-    bt->k1_minb = 2;
-    for (int v = 3; v <= 4; ++v)
-      if (w[v] > w[bt->k1_minb]) bt->k1_minb = v;
-    const char *e = getenv("AFID_K1_VARIANT");
-    if (e && atoi(e) >= 2 && atoi(e) <= 4) bt->k1_minb = atoi(e);
-  }
   c->batches[key] = bt;
   *out = bt;
   return 0;
@@ -356,9 +366,11 @@ BatchDev bdev(const Batch *bt, int fam) {
 int init_kernel_attrs() {
   static bool done = false;
   if (done) return 0;
-  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1>::SMEM));
-  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1>::SMEM));
-  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<2>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 8>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 8>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<2, 8>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<4, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 4>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 2>::SMEM));
   const int fsm = FFT_SMEM_MAX;   // two slots + work + twiddles: (4 N + 4) 16 bytes at one line
   CK(cudaFuncSetAttribute(k_fft_y_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
@@ -421,14 +433,15 @@ int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) 
   k_substep_prep<<<nb, 256, 0, s>>>(bt->d_boxes, nb, ns);
   CKL();
   PMARK(pf, AFID_K_PREP);
-  // variants: 2 = two resident blocks, one plane per barrier; 3 = three
-  // resident blocks; 4 = two resident blocks, two planes per barrier
-  if (bt->k1_minb == 3)
-    k_explicit_implicit_fwd<3, 1><<<bt->total[FAM_K1], 256, K1Ring<1>::SMEM, s>>>(bdev(bt, FAM_K1), ns);
-  else if (bt->k1_minb == 4)
-    k_explicit_implicit_fwd<2, 2><<<bt->total[FAM_K1], 256, K1Ring<2>::SMEM, s>>>(bdev(bt, FAM_K1), ns);
-  else
-    k_explicit_implicit_fwd<2, 1><<<bt->total[FAM_K1], 256, K1Ring<1>::SMEM, s>>>(bdev(bt, FAM_K1), ns);
+  const BatchDev k1 = bdev(bt, FAM_K1);
+  const int nk1 = bt->total[FAM_K1];
+  switch (bt->k1_minb) {
+    case 3: k_explicit_implicit_fwd<8, 3, 1><<<nk1, 256, K1Ring<1, 8>::SMEM, s>>>(k1, ns); break;
+    case 4: k_explicit_implicit_fwd<8, 2, 2><<<nk1, 256, K1Ring<2, 8>::SMEM, s>>>(k1, ns); break;
+    case 5: k_explicit_implicit_fwd<4, 4, 1><<<nk1, 128, K1Ring<1, 4>::SMEM, s>>>(k1, ns); break;
+    case 6: k_explicit_implicit_fwd<2, 8, 1><<<nk1, 64, K1Ring<1, 2>::SMEM, s>>>(k1, ns); break;
+    default: k_explicit_implicit_fwd<8, 2, 1><<<nk1, 256, K1Ring<1, 8>::SMEM, s>>>(k1, ns); break;
+  }
   CKL();
   PMARK(pf, AFID_K_EXPLICIT_FWD);
   k_implicit_bwd<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
@@ -856,7 +869,8 @@ int afid_box_set_tuning(afid_ctx *c, int id, int fft_y_lines, int fft_z_lines, i
     return fail(AFID_EINVAL, "fft_y_lines %d out of range", fft_y_lines);
   if (fft_z_lines < 0 || (fft_z_lines > 0 && !fft_z_ok(d.nzm, fft_z_lines, FFT_SMEM_MAX)))
     return fail(AFID_EINVAL, "fft_z_lines %d out of range", fft_z_lines);
-  if (k1_minb != 0 && (k1_minb < 2 || k1_minb > 4)) return fail(AFID_EINVAL, "k1 variant must be 0, 2, 3 or 4");
+  if (k1_minb != 0 && (k1_minb < K1_VMIN || k1_minb > K1_VMAX))
+    return fail(AFID_EINVAL, "k1 variant must be 0 or %d..%d", K1_VMIN, K1_VMAX);
   rc = set_device(c);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));

@@ -227,13 +227,18 @@ __global__ void k_substep_prep(const BoxDev *__restrict__ boxes, int nbox, int n
   }
 }
 
-constexpr int K1_TJ = 32;
-constexpr int K1_TI = 8;
+constexpr int K1_TJ = 32;                       // tile width along y (one warp)
 constexpr int K1_HJ = K1_TJ + 2;
-constexpr int K1_HI = K1_TI + 2;
-constexpr int K1_PL = K1_HJ * K1_HI;            // one halo plane of one field (340)
-constexpr int K1_NT = K1_TJ * K1_TI;            // threads per block (256)
 constexpr int K1_NTAB = 14;                     // per-k scalars staged per plane
+
+// tile of 32 x TI columns (one warp per row of the tile), halo of one cell
+template <int TI>
+struct K1Shape {
+  static constexpr int HI = TI + 2;
+  static constexpr int PL = K1_HJ * HI;         // one halo plane of one field
+  static constexpr int NT = K1_TJ * TI;         // threads per block
+  static constexpr int NLD = (PL + NT - 1) / NT; // halo elements each thread copies
+};
 
 // per-k scalar slots staged in shared memory
 enum K1Tab { KT_UDX3M = 0, KT_UDX3C, KT_AM3SK, KT_AC3SK, KT_AP3SK, KT_AM3CK, KT_AC3CK, KT_AP3CK,
@@ -248,8 +253,9 @@ struct K1Prev {
 // Accessor over the ring (planes k and k+1, 1-cell halo) and the stash of
 // plane k-1.  Every plane-(k-1) access of the stencil formulas is one of the
 // seven stashed values.
+template <int PL>
 struct RingAcc {
-  const double *ring;   // [slot][field][K1_PL]
+  const double *ring;   // [slot][field][PL]
   int s_c, s_p;         // slots of k and k+1
   int off;              // (ti+1)*K1_HJ + tj+1
   K1Prev prev;
@@ -262,7 +268,7 @@ struct RingAcc {
       return prev.pr;
     }
     const int s = dk > 0 ? s_p : s_c;
-    return ring[(s * F_NF + f) * K1_PL + off + di * K1_HJ + dj];
+    return ring[(s * F_NF + f) * PL + off + di * K1_HJ + dj];
   }
 };
 
@@ -304,20 +310,21 @@ __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int 
 // y(1) = 0 and the missing contribution of its wall row is added by K2 (the
 // solve is linear in y(1)).
 // ---------------------------------------------------------------------------
-template <int PPB>
+template <int PPB, int TI = 8>
 struct K1Ring {
   static constexpr int D = 2 * PPB + 1;        // prefetch distance in planes
   static constexpr int NS = D + PPB;           // ring slots
-  static constexpr int SMEM = (NS * F_NF * K1_PL + NS * 16) * 8;
+  static constexpr int SMEM = (NS * F_NF * K1Shape<TI>::PL + NS * 16) * 8;
 };
 
-template <int MINB, int PPB>
-__global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev bt, int ns) {
-  constexpr int NS = K1Ring<PPB>::NS;
-  constexpr int D = K1Ring<PPB>::D;
+template <int TI, int MINB, int PPB>
+__global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd(BatchDev bt, int ns) {
+  constexpr int NS = K1Ring<PPB, TI>::NS;
+  constexpr int D = K1Ring<PPB, TI>::D;
+  constexpr int PL = K1Shape<TI>::PL, NT = K1Shape<TI>::NT, NLD = K1Shape<TI>::NLD;
   extern __shared__ double k1sm[];
   double *ring = k1sm;
-  double *tring = k1sm + NS * F_NF * K1_PL;      // [slot][16]
+  double *tring = k1sm + NS * F_NF * PL;         // [slot][16]
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
@@ -328,7 +335,7 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
   const int nym = B.nym, nzm = B.nzm;
   const int ntj = (nym + K1_TJ - 1) / K1_TJ;
   const int j0 = (tile % ntj) * K1_TJ;
-  const int i0 = (tile / ntj) * K1_TI;
+  const int i0 = (tile / ntj) * TI;
   const int tj = tid % K1_TJ;
   const int ti = tid / K1_TJ;
   const int j = j0 + tj, i = i0 + ti;
@@ -345,29 +352,25 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
 
   const double *fld[F_NF] = {B.vx, B.vy, B.vz, B.temp, B.pr};
 
-  // this thread's halo elements (r0 = tid always < K1_PL; r1 = tid + K1_NT if < K1_PL)
-  const int r1 = tid + K1_NT;
-  const bool has1 = r1 < K1_PL;
-  long long g0, g1 = 0;
-  {
-    int hi = tid / K1_HJ, hj = tid - hi * K1_HJ;
-    int jj = (j0 + hj - 1 + nym) % nym, ii = (i0 + hi - 1 + nzm) % nzm;
-    g0 = (long long)ii * nym + jj;
-    if (has1) {
-      hi = r1 / K1_HJ; hj = r1 - hi * K1_HJ;
-      jj = (j0 + hj - 1 + nym) % nym; ii = (i0 + hi - 1 + nzm) % nzm;
-      g1 = (long long)ii * nym + jj;
-    }
+  // this thread's halo elements: r = tid + q NT for q < NLD while r < PL
+  long long g[NLD];
+#pragma unroll
+  for (int q = 0; q < NLD; ++q) {
+    const int r = tid + q * NT;
+    const int hi = r / K1_HJ, hj = r - hi * K1_HJ;
+    const int jj = (j0 + hj - 1 + nym) % nym, ii = (i0 + hi - 1 + nzm) % nzm;
+    g[q] = (long long)ii * nym + jj;
   }
   auto load_plane = [&](int p) {      // plane p and its per-k scalars into slot p % NS
     if (p > nx - 1) return;
     const int sl = p % NS;
-    double *dst = ring + sl * F_NF * K1_PL;
+    double *dst = ring + sl * F_NF * PL;
     const long long po = (long long)p * P;
 #pragma unroll
     for (int f = 0; f < F_NF; ++f) {
-      cp_async8(dst + f * K1_PL + tid, fld[f] + po + g0);
-      if (has1) cp_async8(dst + f * K1_PL + r1, fld[f] + po + g1);
+#pragma unroll
+      for (int q = 0; q < NLD; ++q)
+        if (q * NT + tid < PL) cp_async8(dst + f * PL + tid + q * NT, fld[f] + po + g[q]);
     }
     if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + sl * 16 + tid, k1_tab_src(B, tid, p));
   };
@@ -378,7 +381,7 @@ __global__ void __launch_bounds__(K1_NT, MINB) k_explicit_implicit_fwd(BatchDev 
     }
   };
 
-  RingAcc acc;
+  RingAcc<PL> acc;
   acc.ring = ring;
   acc.off = (ti + 1) * K1_HJ + tj + 1;
   acc.prev = K1Prev{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};

@@ -94,18 +94,20 @@ def test_fft_size_rule(ctx):
         ctx.add_box(cfg_of(16, 22, 16))
 
 
-def test_launch_shapes_do_not_change_results(ctx):
-    """Tuned launch shapes (FFT lines per block, explicit-kernel occupancy
-    variant) give bit-identical fields."""
+@pytest.mark.parametrize("fy,fz,k1", [(1, 2, 3), (2, 1, 4), (4, 4, 5), (2, 8, 6)])
+def test_launch_shapes_do_not_change_results(ctx, fy, fz, k1):
+    """Tuned launch shapes (FFT lines per block, tile shape and occupancy of
+    the explicit kernel) give bit-identical fields."""
     a = _add(ctx, MIX[2], 21)
     b = _add(ctx, MIX[2], 21)
-    b.set_tuning(fft_y_lines=1, fft_z_lines=2, k1_minb=3)
+    b.set_tuning(fft_y_lines=fy, fft_z_lines=fz, k1_minb=k1)
     ctx.step([a], 3)
     ctx.step([b], 3)
     for f in FIELDS:
         assert np.array_equal(a.download(f), b.download(f)), f
     from afid_b200._lib import AfidError
-    with pytest.raises(AfidError):
-        b.set_tuning(fft_y_lines=10 ** 6)
+    for bad in (dict(fft_y_lines=10 ** 6), dict(fft_y_lines=3), dict(fft_z_lines=6), dict(k1_minb=7)):
+        with pytest.raises(AfidError):
+            b.set_tuning(**bad)
     for x in (a, b):
         ctx.remove_box(x)
