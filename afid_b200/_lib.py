@@ -34,7 +34,12 @@ EXPORTS = [
     "afid_calc_max_cfl", "afid_check_divergence", "afid_calc_plate_nu", "afid_step",
     "afid_step_graph", "afid_substep", "afid_step_profiled",
     "afid_solve_pressure_correction_noalloc", "afid_box_set_tuning",
+    "afid_global_quantities", "afid_calc_stats", "afid_calc_dissipation_nu", "afid_box_get_stats",
+    "afid_box_reset_stats", "afid_slab_locations", "afid_slab_dump",
 ]
+
+STATS = ["vx_me", "vy_me", "vz_me", "temp_me", "vx_rms", "vy_rms", "vz_rms", "temp_rms", "tempvx_me",
+         "disste", "dissth"]
 
 KERNELS = ["diag", "finalize", "prep", "explicit_fwd", "implicit_bwd", "fft_y_fwd", "fft_z_fwd",
            "poisson_x", "fft_z_inv", "fft_y_inv", "correct", "plate_nu", "divergence"]
@@ -50,6 +55,14 @@ class BoxParams(C.Structure):
         ("dt", C.c_double), ("idtv", C.c_int),
         ("cflmax", C.c_double), ("dtmin", C.c_double), ("dtmax", C.c_double),
         ("vlim", C.c_double), ("resid", C.c_double),
+    ]
+
+
+class GlobalQ(C.Structure):
+    _fields_ = [
+        ("nu_vol", C.c_double), ("vmax", C.c_double * 3), ("tempm", C.c_double),
+        ("tempmax", C.c_double), ("tempmin", C.c_double), ("vz_rms", C.c_double),
+        ("vy_rms", C.c_double), ("vx_rms", C.c_double), ("vel_rms", C.c_double),
     ]
 
 
@@ -108,6 +121,13 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_step_profiled": ([vp, ip, i, i, dp, ip, i], i),
         "afid_solve_pressure_correction_noalloc": ([vp, i, i, i, dp, d, d, d, vp], i),
         "afid_box_set_tuning": ([vp, i, i, i, i], i),
+        "afid_global_quantities": ([vp, i, C.POINTER(GlobalQ)], i),
+        "afid_calc_stats": ([vp, i], i),
+        "afid_calc_dissipation_nu": ([vp, i, dp, dp], i),
+        "afid_box_get_stats": ([vp, i, dp, ip], i),
+        "afid_box_reset_stats": ([vp, i], i),
+        "afid_slab_locations": ([i, dp, dp, ip], i),
+        "afid_slab_dump": ([vp, i, ip, i, dp], i),
     }
     for name in ("explicit_terms_vx", "explicit_terms_vy", "explicit_terms_vz",
                  "explicit_terms_temp", "implicit_and_update_vx", "implicit_and_update_vy",

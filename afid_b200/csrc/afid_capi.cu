@@ -57,6 +57,11 @@ struct HostBox {
   BoxDev *d_self = nullptr;  // device copy of dev (active = 1), for single-box kernels
   void *mem_fields = nullptr, *mem_scratch = nullptr, *mem_small = nullptr, *mem_routine = nullptr;
   size_t scratch_doubles = 0;
+  std::vector<double> xc;                // node positions (host copy, for the output diagnostics)
+  double *d_out = nullptr;               // device staging of the output diagnostics (grown on demand)
+  size_t out_doubles = 0;
+  std::vector<double> stats;             // AFID_NSTAT x nxm accumulators (stat_arrays)
+  int nstatsamples = 0;
 };
 
 struct Batch {
@@ -718,6 +723,8 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
     return fail(AFID_ECUDA, "box_add: initialisation copy failed");
   }
   hb->id = c->next_id++;
+  hb->xc.assign(xc, xc + p->nxm + 1);
+  hb->stats.assign((size_t)AFID_NSTAT * p->nxm, 0.0);
   rc = sync_self(hb);
   if (rc) return rc;
   c->boxes[hb->id] = hb;
@@ -739,7 +746,7 @@ int afid_box_remove(afid_ctx *c, int id) {
     else ++it;
   }
   cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small);
-  cudaFree(hb->mem_routine); cudaFree(hb->d_self);
+  cudaFree(hb->mem_routine); cudaFree(hb->d_self); cudaFree(hb->d_out);
   c->boxes.erase(id);
   delete hb;
   return 0;
@@ -1118,6 +1125,201 @@ int afid_step_graph(afid_ctx *c, const int *ids, int n, int nsteps) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Output-time diagnostics (main.F90:202-216): GlobalQuantities, CalcStats,
+// CalcDissipationNu and SlabDumper.  One kernel computes the per-plane sums
+// and extrema of all of them; the host adds the chunks of each plane and the
+// planes in a fixed order, so results do not depend on scheduling.
+// ============================================================================
+namespace {
+
+int ensure_out(HostBox *hb, size_t doubles) {
+  if (hb->out_doubles >= doubles) return 0;
+  cudaFree(hb->d_out);
+  hb->d_out = nullptr;
+  hb->out_doubles = 0;
+  if (cudaMalloc(&hb->d_out, doubles * sizeof(double)) != cudaSuccess)
+    return fail(AFID_ENOMEM, "diagnostics staging of %zu doubles", doubles);
+  hb->out_doubles = doubles;
+  return 0;
+}
+
+// per-plane sums (q < PQ_NSUM) and extrema of box id, pl[k * PQ_N + q]
+int plane_sums(afid_ctx *c, int id, HostBox **phb, std::vector<double> &pl) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (!rc) rc = set_device(c);
+  if (rc) return rc;
+  const int nxm = hb->dev.nxm;
+  const size_t n = (size_t)nxm * PS_CHUNKS * PQ_N;
+  rc = ensure_out(hb, n);
+  if (rc) return rc;
+  k_plane_sums<<<dim3(PS_CHUNKS, nxm), 256, 0, c->stream>>>(hb->d_self, hb->d_out);
+  CKL();
+  std::vector<double> raw(n);
+  CK(cudaMemcpyAsync(raw.data(), hb->d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  pl.assign((size_t)nxm * PQ_N, 0.0);
+  for (int k = 0; k < nxm; ++k)
+    for (int q = 0; q < PQ_N; ++q) {
+      double v = raw[((size_t)k * PS_CHUNKS) * PQ_N + q];
+      for (int ch = 1; ch < PS_CHUNKS; ++ch) {
+        const double u = raw[((size_t)k * PS_CHUNKS + ch) * PQ_N + q];
+        v = q < PQ_NSUM ? v + u : std::max(v, u);
+      }
+      pl[(size_t)k * PQ_N + q] = v;
+    }
+  *phb = hb;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int afid_global_quantities(afid_ctx *c, int id, afid_global_q *out) {
+  if (!out) return fail(AFID_EINVAL, "null output");
+  HostBox *hb;
+  std::vector<double> pl;
+  int rc = plane_sums(c, id, &hb, pl);
+  if (rc) return rc;
+  const afid_box_params &p = hb->prm;
+  const int nxm = p.nxm;
+  const double *xc = hb->xc.data();
+  const double dx = (double)nxm / p.alx3;
+  double anusin = 0, tempm = 0, vxr = 0, vyr = 0, vzr = 0, vall = 0;
+  double vmz = 0, vmy = 0, vmx = 0, tmax = -1.7976931348623157e308, tmin = 1.7976931348623157e308;
+  for (int k = 0; k < nxm; ++k) {
+    // fac2 = g3rc(kc) (CreateGrid.F90:143-150)
+    const double fac2 = k == 0 ? (xc[1] - xc[0]) * dx : (xc[k + 1] - xc[k - 1]) * dx * 0.5;
+    const double *q = &pl[(size_t)k * PQ_N];
+    anusin += q[PQ_TCVXC] * fac2;
+    tempm += q[PQ_TC] * fac2;
+    vxr += q[PQ_VX2] * fac2;
+    vyr += q[PQ_VY2] * fac2;
+    vzr += q[PQ_VZ2] * fac2;
+    vall += (q[PQ_VZ2] + q[PQ_VY2] + q[PQ_VX2]) * fac2;
+    vmz = std::max(vmz, q[PQ_MAXVZ]);
+    vmy = std::max(vmy, q[PQ_MAXVY]);
+    vmx = std::max(vmx, q[PQ_MAXVX]);
+    tmax = std::max(tmax, q[PQ_MAXT]);
+    tmin = std::min(tmin, -q[PQ_NEGMINT]);
+  }
+  const double vol = 1.0 / (p.alx3 * dx * (double)p.nzm * (double)p.nym);
+  const double rradpr = std::sqrt(p.ray / p.pra);
+  out->nu_vol = 1.0 + std::sqrt(p.pra * p.ray) * anusin * vol;
+  out->vmax[0] = vmz;
+  out->vmax[1] = vmy;
+  out->vmax[2] = vmx;
+  out->tempm = tempm * vol;
+  out->tempmax = tmax;
+  out->tempmin = tmin;
+  out->vz_rms = std::sqrt(vzr * vol) * rradpr;
+  out->vy_rms = std::sqrt(vyr * vol) * rradpr;
+  out->vx_rms = std::sqrt(vxr * vol) * rradpr;
+  out->vel_rms = std::sqrt(vall * vol) * rradpr;
+  return 0;
+}
+
+extern "C" int afid_calc_stats(afid_ctx *c, int id) {
+  HostBox *hb;
+  std::vector<double> pl;
+  int rc = plane_sums(c, id, &hb, pl);
+  if (rc) return rc;
+  const int nxm = hb->prm.nxm;
+  const double usnym = 1.0 / hb->prm.nym, usnzm = 1.0 / hb->prm.nzm;
+  static const int src[9] = {PQ_VX, PQ_VY, PQ_VZ, PQ_T, PQ_VX2, PQ_VY2, PQ_VZ2, PQ_T2, PQ_TVX};
+  for (int a = 0; a < 9; ++a)
+    for (int k = 0; k < nxm; ++k) hb->stats[(size_t)a * nxm + k] += pl[(size_t)k * PQ_N + src[a]] * usnzm * usnym;
+  hb->nstatsamples += 1;
+  return 0;
+}
+
+extern "C" int afid_calc_dissipation_nu(afid_ctx *c, int id, double *nu_mu, double *nu_th) {
+  if (!nu_mu || !nu_th) return fail(AFID_EINVAL, "null output");
+  HostBox *hb;
+  std::vector<double> pl;
+  int rc = plane_sums(c, id, &hb, pl);
+  if (rc) return rc;
+  const afid_box_params &p = hb->prm;
+  const int nxm = p.nxm;
+  const double *xc = hb->xc.data();
+  const double dx = (double)nxm / p.alx3;
+  const double ren = std::sqrt(p.ray / p.pra), pec = std::sqrt(p.pra * p.ray);
+  auto xm = [&](int k) { return (xc[k] + xc[k + 1]) * 0.5; };
+  double mu = 0.0, th = 0.0;
+  for (int k = 0; k < nxm; ++k) {
+    // lem, lec of CalcDissipationNu.F90:32-40
+    const double lem = (xc[k + 1] - xc[k]) * dx;
+    const double lec = k < nxm - 1 ? (xm(k + 1) - xm(k)) * dx : (xm(nxm - 1) - xm(nxm - 2)) * dx;
+    const double *q = &pl[(size_t)k * PQ_N];
+    mu += q[PQ_DISSTE] * lem * p.pra + q[PQ_DISSTE2] * lec * p.pra;
+    th += q[PQ_DISSTH] * lem;
+    hb->stats[(size_t)AFID_STAT_DISSTE * nxm + k] +=
+        (q[PQ_DISSTE] + q[PQ_DISSTE2]) / (ren * (double)p.nym * (double)p.nzm);
+    hb->stats[(size_t)AFID_STAT_DISSTH * nxm + k] += q[PQ_DISSTH] / (pec * (double)p.nym * (double)p.nzm);
+  }
+  const double volt = 1.0 / ((double)nxm * (double)p.nzm * (double)p.nym);
+  *nu_mu = mu * volt + 1.0;
+  *nu_th = th * volt;
+  return 0;
+}
+
+extern "C" int afid_box_get_stats(afid_ctx *c, int id, double *out, int *nsamples) {
+  if (!c || !out) return fail(AFID_EINVAL, "null argument");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  std::copy(hb->stats.begin(), hb->stats.end(), out);
+  if (nsamples) *nsamples = hb->nstatsamples;
+  return 0;
+}
+
+extern "C" int afid_box_reset_stats(afid_ctx *c, int id) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  std::fill(hb->stats.begin(), hb->stats.end(), 0.0);
+  hb->nstatsamples = 0;
+  return 0;
+}
+
+extern "C" int afid_slab_locations(int nxm, const double *xc, const double *xslab, int *kslab) {
+  if (!xc || !xslab || !kslab || nxm < 3) return fail(AFID_EINVAL, "slab_locations: bad argument");
+  // InitializeSlabDump (SlabDumpRoutines.F90:52-67): kslab(1) = 2; slab m
+  // = 2..9 at the last k in 2..nxm with xm(k-1) < xslab(m) < xm(k)
+  auto xm = [&](int k1) { return (xc[k1 - 1] + xc[k1]) * 0.5; };   // 1-based xm(k)
+  for (int m = 0; m < 9; ++m) kslab[m] = 2;
+  for (int k = 2; k <= nxm; ++k)
+    for (int m = 2; m <= 9; ++m)
+      if (xm(k) > xslab[m - 2] && xm(k - 1) < xslab[m - 2]) kslab[m - 1] = k;
+  return 0;
+}
+
+extern "C" int afid_slab_dump(afid_ctx *c, int id, const int *kslab, int nslab, double *out) {
+  if (!c || !kslab || !out || nslab < 1 || nslab > 16) return fail(AFID_EINVAL, "slab_dump: 1..16 slabs");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (!rc) rc = set_device(c);
+  if (rc) return rc;
+  SlabList sl;
+  for (int m = 0; m < nslab; ++m) {
+    if (kslab[m] < 1 || kslab[m] > hb->prm.nxm)
+      return fail(AFID_EINVAL, "slab_dump: kslab %d outside 1..nxm", kslab[m]);
+    sl.k[m] = kslab[m] - 1;
+  }
+  const long long P = hb->dev.plane;
+  const size_t n = (size_t)nslab * 4 * P;
+  rc = ensure_out(hb, n);
+  if (rc) return rc;
+  k_slab_gather<<<dim3((unsigned)std::min<long long>(cdiv(P, 256), 1024), nslab), 256, 0, c->stream>>>(
+      hb->d_self, sl, nslab, hb->d_out);
+  CKL();
+  CK(cudaMemcpyAsync(out, hb->d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
 
 // ============================================================================
 // Pressure solve without allocation.

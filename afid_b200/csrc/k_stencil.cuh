@@ -823,6 +823,110 @@ __global__ void __launch_bounds__(256) k_plate_nu(const BoxDev *__restrict__ box
   if (threadIdx.x == 0) { B.nu_part[2 * blockIdx.x] = s_lo[0]; B.nu_part[2 * blockIdx.x + 1] = s_up[0]; }
 }
 
+// ---------------------------------------------------------------------------
+// Output-time diagnostics: per-plane horizontal sums and extrema of
+// GlobalQuantities.F90:38-61, CalcStats (StatRoutines.F90:21-43) and
+// CalcDissipationNu.F90:53-105, all in one pass over vx, vy, vz, temp.
+// Block (c, k) reduces chunk c of the columns of plane k (k = 0..nxm-1,
+// reading plane k+1 and the j+1, i+1 neighbours); the host adds the chunks
+// of a plane in a fixed order and weights the planes.
+// ---------------------------------------------------------------------------
+enum PlaneQ {
+  PQ_VX, PQ_VY, PQ_VZ, PQ_T, PQ_VX2, PQ_VY2, PQ_VZ2, PQ_T2, PQ_TVX,  // CalcStats
+  PQ_TCVXC, PQ_TC,                                                  // GlobalQuantities
+  PQ_DISSTE, PQ_DISSTE2, PQ_DISSTH,                                 // CalcDissipationNu
+  PQ_NSUM,                                                          // sums above, maxima below
+  PQ_MAXVZ = PQ_NSUM, PQ_MAXVY, PQ_MAXVX, PQ_MAXT, PQ_NEGMINT, PQ_N
+};
+constexpr int PS_CHUNKS = 16;
+
+__global__ void __launch_bounds__(256) k_plane_sums(const BoxDev *__restrict__ bp, double *__restrict__ out) {
+  const BoxDev &B = *bp;
+  const int k = blockIdx.y, c = blockIdx.x;
+  const int nym = B.nym, nzm = B.nzm, nxm = B.nxm;
+  const long long P = B.plane;
+  const double *xc = B.tab + (long long)T_XC * B.nx;
+  // CalcDissipationNu.F90:32-40: dxc(k), and dxm(k) with the last plane
+  // reusing the spacing of the cell centres below it
+  const double dxc = 1.0 / (xc[k + 1] - xc[k]);
+  const int km = k < nxm - 1 ? k : nxm - 2;
+  const double dxm = 1.0 / ((xc[km + 1] + xc[km + 2]) * 0.5 - (xc[km] + xc[km + 1]) * 0.5);
+  const double dy = B.dy, dz = B.dz;
+  double s[PQ_N];
+#pragma unroll
+  for (int q = 0; q < PQ_N; ++q) s[q] = 0.0;
+  s[PQ_MAXT] = -1.7976931348623157e308;
+  s[PQ_NEGMINT] = -1.7976931348623157e308;
+  const double *vx = B.vx + (long long)k * P, *vy = B.vy + (long long)k * P;
+  const double *vz = B.vz + (long long)k * P, *tp = B.temp + (long long)k * P;
+  for (long long col = (long long)c * blockDim.x + threadIdx.x; col < P; col += (long long)PS_CHUNKS * blockDim.x) {
+    const int i = (int)(col / nym), j = (int)(col - (long long)i * nym);
+    const long long oj = (long long)i * nym + (j == nym - 1 ? 0 : j + 1);
+    const long long oi = (long long)(i == nzm - 1 ? 0 : i + 1) * nym + j;
+    const double vx0 = vx[col], vx1 = vx[col + P], vxj = vx[oj], vxi = vx[oi];
+    const double vy0 = vy[col], vy1 = vy[col + P], vyj = vy[oj], vyi = vy[oi];
+    const double vz0 = vz[col], vz1 = vz[col + P], vzj = vz[oj], vzi = vz[oi];
+    const double t0 = tp[col], t1 = tp[col + P], tj = tp[oj], ti = tp[oi];
+    s[PQ_VX] += vx0; s[PQ_VY] += vy0; s[PQ_VZ] += vz0; s[PQ_T] += t0;
+    s[PQ_VX2] += vx0 * vx0; s[PQ_VY2] += vy0 * vy0; s[PQ_VZ2] += vz0 * vz0; s[PQ_T2] += t0 * t0;
+    s[PQ_TVX] += t0 * vx0;
+    const double vxcen = (vx0 + vx1) * 0.5, tempcen = (t0 + t1) * 0.5;
+    s[PQ_TCVXC] += tempcen * vxcen;
+    s[PQ_TC] += tempcen;
+    const double hxx = (vx1 - vx0) * dxc, hxy = (vxj - vx0) * dy, hxz = (vxi - vx0) * dz;
+    const double hyx = (vy1 - vy0) * dxm, hyy = (vyj - vy0) * dy, hyz = (vyi - vy0) * dz;
+    const double hzx = (vz1 - vz0) * dxm, hzy = (vzj - vz0) * dy, hzz = (vzi - vz0) * dz;
+    s[PQ_DISSTE] += hxx * hxx + hxy * hxy + hxz * hxz;
+    s[PQ_DISSTE2] += (hyx * hyx + hyy * hyy + hyz * hyz) + (hzx * hzx + hzy * hzy + hzz * hzz);
+    const double tx = (t1 - t0) * dxc, ty = (tj - t0) * dy, tz = (ti - t0) * dz;
+    s[PQ_DISSTH] += tx * tx + ty * ty + tz * tz;
+    s[PQ_MAXVZ] = fmax(s[PQ_MAXVZ], fabs(vz0));
+    s[PQ_MAXVY] = fmax(s[PQ_MAXVY], fabs(vy0));
+    s[PQ_MAXVX] = fmax(s[PQ_MAXVX], fabs(vx0));
+    s[PQ_MAXT] = fmax(s[PQ_MAXT], t0);
+    s[PQ_NEGMINT] = fmax(s[PQ_NEGMINT], -t0);
+  }
+  __shared__ double red[8][PQ_N];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < PQ_N; ++q) {
+    double v = s[q];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, v, o);
+      v = q < PQ_NSUM ? v + u : fmax(v, u);
+    }
+    if (l == 0) red[w][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < PQ_N) {
+    const int q = threadIdx.x;
+    double v = red[0][q];
+    for (int x = 1; x < (int)(blockDim.x >> 5); ++x) v = q < PQ_NSUM ? v + red[x][q] : fmax(v, red[x][q]);
+    out[((long long)k * PS_CHUNKS + c) * PQ_N + q] = v;
+  }
+}
+
+// Horizontal slabs of SlabDumper (SlabDumpRoutines.F90:15-24): for slab m
+// at plane kslab[m] (0-based), (vx(k) + vx(k+1)) / 2, vy(k), vz(k), temp(k)
+// into out[m][4][plane].
+struct SlabList {
+  int k[16];
+};
+__global__ void k_slab_gather(const BoxDev *__restrict__ bp, SlabList sl, int nslab, double *__restrict__ out) {
+  const BoxDev &B = *bp;
+  const long long P = B.plane;
+  const int m = blockIdx.y;
+  if (m >= nslab) return;
+  const long long o = (long long)sl.k[m] * P;
+  double *dst = out + (long long)m * 4 * P;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P; c += (long long)gridDim.x * blockDim.x) {
+    dst[c] = (B.vx[o + c] + B.vx[o + P + c]) * 0.5;
+    dst[P + c] = B.vy[o + c];
+    dst[2 * P + c] = B.vz[o + c];
+    dst[3 * P + c] = B.temp[o + c];
+  }
+}
+
 // Finalise the reductions of one box (thread per box): diagnostics, plate Nu
 // and the reference's error codes.
 //   mode 0: step start  -> cfl/div/vmax from k_diag, then the dt rule of

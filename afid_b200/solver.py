@@ -28,6 +28,19 @@ def make_grid(nxm: int, istr3: int = 7, str3: float = 0.0, alx3: float = 1.0) ->
     return xc
 
 
+def slab_locations(xc: np.ndarray, xslab) -> list[int]:
+    """kslab(1..9) of InitializeSlabDump from the eight x positions of
+    stst3.in (1-based planes), computed by the library."""
+    nxm = len(xc) - 1
+    xs = np.ascontiguousarray(xslab, dtype=np.float64)
+    if xs.shape != (8,):
+        raise ValueError("xslab holds the eight positions of slabs 2..9")
+    ks = np.zeros(9, dtype=np.int32)
+    _lib.check(_lib.lib().afid_slab_locations(nxm, _lib.dptr(np.ascontiguousarray(xc, dtype=np.float64)),
+                                              _lib.dptr(xs), ks.ctypes.data_as(C.POINTER(C.c_int))))
+    return [int(k) for k in ks]
+
+
 def box_params(cfg: BouIn) -> _lib.BoxParams:
     p = _lib.BoxParams()
     for name in ("nxm", "nym", "nzm", "nsst", "alx3", "ylen", "zlen", "ray", "pra", "inslws",
@@ -214,6 +227,51 @@ class Box:
         a, b = C.c_double(), C.c_double()
         _lib.check(self._L.afid_calc_plate_nu(self.ctx.h, self.id, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    # ---- output-time diagnostics (main.F90:202-216) ----------------------
+    def global_quantities(self) -> dict:
+        """GlobalQuantities.F90: volume Nu, max |v|, temperature mean and
+        extrema, rms velocities (times sqrt(Ra/Pr))."""
+        q = _lib.GlobalQ()
+        _lib.check(self._L.afid_global_quantities(self.ctx.h, self.id, C.byref(q)))
+        return dict(nu_vol=q.nu_vol, vmax=tuple(q.vmax), tempm=q.tempm, tempmax=q.tempmax,
+                    tempmin=q.tempmin, vz_rms=q.vz_rms, vy_rms=q.vy_rms, vx_rms=q.vx_rms,
+                    vel_rms=q.vel_rms)
+
+    def calc_stats(self):
+        """CalcStats (StatRoutines.F90): add this state's horizontal means to
+        the box's profiles."""
+        _lib.check(self._L.afid_calc_stats(self.ctx.h, self.id))
+
+    def calc_dissipation_nu(self) -> tuple[float, float]:
+        """CalcDissipationNu.F90: (nu_mu, nu_th); adds the dissipation
+        profiles to the box's disste and dissth."""
+        a, b = C.c_double(), C.c_double()
+        _lib.check(self._L.afid_calc_dissipation_nu(self.ctx.h, self.id, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def stats(self) -> dict:
+        """Accumulated profiles (one array of nxm per name) and nstatsamples."""
+        nxm = self.cfg.nxm
+        buf = np.zeros(len(_lib.STATS) * nxm)
+        n = C.c_int()
+        _lib.check(self._L.afid_box_get_stats(self.ctx.h, self.id, _lib.dptr(buf), C.byref(n)))
+        out = {name: buf[q * nxm:(q + 1) * nxm].copy() for q, name in enumerate(_lib.STATS)}
+        out["nstatsamples"] = n.value
+        return out
+
+    def reset_stats(self):
+        _lib.check(self._L.afid_box_reset_stats(self.ctx.h, self.id))
+
+    def slab_dump(self, kslab) -> np.ndarray:
+        """SlabDumper: for each 1-based plane k of ``kslab``, the slabs
+        (vx(k)+vx(k+1))/2, vy(k), vz(k), temp(k); array (n, 4, nym, nzm)."""
+        ks = np.ascontiguousarray(kslab, dtype=np.int32)
+        c = self.cfg
+        buf = np.empty((len(ks), 4, c.nzm, c.nym))
+        _lib.check(self._L.afid_slab_dump(self.ctx.h, self.id, ks.ctypes.data_as(C.POINTER(C.c_int)),
+                                          len(ks), _lib.dptr(buf)))
+        return np.ascontiguousarray(buf.transpose(0, 1, 3, 2))
 
     def time_marcher_routines(self):
         """One TimeMarcher step (TimeMarcher.F90:24-74) through the

@@ -39,14 +39,14 @@ sys.path.insert(0, ROOT)
 METRIC = "Mpoint-steps/s FP64 (RK3 step, cells = nxm*nym*nzm)"
 UNIT = "Mpoint-steps/s"
 
-# DRAM traffic per cell of each kernel, dram__bytes_read.sum +
-# dram__bytes_write.sum / (nxm*nym*nzm), from the ncu --set full capture of
-# the 193x384x384 box summarised in profiles/ncu_full_substep_193x384x384.md
-# (traffic scales with the number of cells; the kernels have the same
-# per-cell structure at every size).
+# DRAM traffic per cell of each kernel, (dram__bytes_read.sum +
+# dram__bytes_write.sum) / (nxm*nym*nzm), from one ncu --set full capture of
+# the 193x384x384 box (bench.py --workload s384, one step); traffic scales with
+# the number of cells, the kernels having the same per-cell structure at every
+# size.
 NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
-    "explicit_fwd": 135.8, "implicit_bwd": 94.5, "fft_z_fwd": 14.3,
-    "poisson_x": 34.0, "fft_z_inv": 14.3, "fft_y_inv": 14.6,
+    "explicit_fwd": 135.4, "implicit_bwd": 95.1, "divergence": 36.4, "fft_y_fwd": 14.4,
+    "fft_z_fwd": 14.5, "poisson_x": 33.9, "fft_z_inv": 14.5, "fft_y_inv": 14.6, "diag": 32.4,
 }
 
 

@@ -191,6 +191,37 @@ enum afid_kernel {
 int afid_step_profiled(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps,
                        double *kernel_ms, int *kernel_launches, int nkernel);
 
+/* ---- output-time diagnostics (main.F90:202-216) ---------------------------
+ * Called between steps at output times, as main.F90 does.  Each call reads
+ * the box's current vx, vy, vz and temp once on the device; sums run in a
+ * fixed order (results do not depend on scheduling). */
+typedef struct afid_global_q {
+  double nu_vol;          /* 1 + sqrt(Pr Ra) <T vx> (nu_vol.out) */
+  double vmax[3];         /* max |vz|, |vy|, |vx| */
+  double tempm, tempmax, tempmin;
+  double vz_rms, vy_rms, vx_rms, vel_rms;   /* rms_vel.out, times sqrt(Ra/Pr) */
+} afid_global_q;
+int afid_global_quantities(afid_ctx *ctx, int box_id, afid_global_q *out);  /* GlobalQuantities.F90:11 */
+/* Profiles accumulated per box (module stat_arrays), AFID_NSTAT x nxm values,
+ * profile by profile: CalcStats adds the first nine and increments the
+ * sample count; CalcDissipationNu adds disste and dissth. */
+enum afid_stat {
+  AFID_STAT_VX_ME = 0, AFID_STAT_VY_ME, AFID_STAT_VZ_ME, AFID_STAT_TEMP_ME,
+  AFID_STAT_VX_RMS, AFID_STAT_VY_RMS, AFID_STAT_VZ_RMS, AFID_STAT_TEMP_RMS,
+  AFID_STAT_TEMPVX_ME, AFID_STAT_DISSTE, AFID_STAT_DISSTH, AFID_NSTAT
+};
+int afid_calc_stats(afid_ctx *ctx, int box_id);                               /* StatRoutines.F90:12 */
+int afid_calc_dissipation_nu(afid_ctx *ctx, int box_id, double *nu_mu, double *nu_th); /* CalcDissipationNu.F90:11 */
+int afid_box_get_stats(afid_ctx *ctx, int box_id, double *out, int *nstatsamples);
+int afid_box_reset_stats(afid_ctx *ctx, int box_id);
+/* kslab(1..9) of InitializeSlabDump (SlabDumpRoutines.F90:42-67) from the
+ * eight x positions of stst3.in (host only, 1-based k). */
+int afid_slab_locations(int nxm, const double *xc, const double *xslab, int *kslab);
+/* SlabDumper (SlabDumpRoutines.F90:11-35): for each of nslab (<= 16) 1-based
+ * planes, (vx(k)+vx(k+1))/2, vy(k), vz(k), temp(k) as nym x nzm arrays in
+ * (j, i) order: out holds nslab*4*nym*nzm doubles. */
+int afid_slab_dump(afid_ctx *ctx, int box_id, const int *kslab, int nslab, double *out);
+
 /* ---- pressure solve without allocation ------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory while they run (memory handed to their own pool, code paths where

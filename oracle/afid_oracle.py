@@ -857,7 +857,106 @@ def global_quantities(s: State):
         tempm=tempm * vol, tempmax=float(s.temp[kc].max()),
         tempmin=float(s.temp[kc].min()),
         vx_rms=math.sqrt(vxr * vol) * rr, vy_rms=math.sqrt(vyr * vol) * rr,
-        vz_rms=math.sqrt(vzr * vol) * rr)
+        vz_rms=math.sqrt(vzr * vol) * rr,
+        vel_rms=math.sqrt((vzr + vyr + vxr) * vol) * rr)
+
+
+def dissipation_metrics(g: Grid, nxm: int):
+    """dxm, dxc, lem, lec of CalcDissipationNu.F90:32-40 (0-based k)."""
+    xm, xc, dx = g.xm, g.xc, g.dx
+    dxm = np.empty(nxm)
+    dxc = np.empty(nxm)
+    lem = np.empty(nxm)
+    lec = np.empty(nxm)
+    for k in range(nxm):
+        dxm[k] = 1.0 / (xm[k + 1] - xm[k]) if k < nxm - 1 else 0.0
+        dxc[k] = 1.0 / (xc[k + 1] - xc[k])
+        lem[k] = (xc[k + 1] - xc[k]) * dx
+        lec[k] = (xm[k + 1] - xm[k]) * dx
+    lec[nxm - 1] = (xm[nxm - 1] - xm[nxm - 2]) * dx
+    dxm[nxm - 1] = 1.0 / (xm[nxm - 1] - xm[nxm - 2])
+    return dxm, dxc, lem, lec
+
+
+def calc_dissipation_nu(s: State):
+    """Nusselt numbers from the viscous and thermal dissipation rates and
+    their per-plane profiles (CalcDissipationNu.F90:42-117).  Returns nu_mu,
+    nu_th and the per-plane increments of the disste and dissth
+    accumulators (the stat arrays of the reference)."""
+    p, g = s.p, s.g
+    nxm, nym, nzm = p.nxm, p.nym, p.nzm
+    dxm, dxc, lem, lec = dissipation_metrics(g, nxm)
+    kc, kp = slice(0, nxm), slice(1, nxm + 1)
+    c3 = (slice(None), None, None)
+    vx, vy, vz, t = s.vx[kc], s.vy[kc], s.vz[kc], s.temp[kc]
+    hxx = (s.vx[kp] - vx) * dxc[c3]
+    hxy = (_jp(vx) - vx) * g.dy
+    hxz = (_ip(vx) - vx) * g.dz
+    hyx = (s.vy[kp] - vy) * dxm[c3]
+    hyy = (_jp(vy) - vy) * g.dy
+    hyz = (_ip(vy) - vy) * g.dz
+    hzx = (s.vz[kp] - vz) * dxm[c3]
+    hzy = (_jp(vz) - vz) * g.dy
+    hzz = (_ip(vz) - vz) * g.dz
+    dissipte = hxx * hxx + hxy * hxy + hxz * hxz
+    dissipte2 = (hyx * hyx + hyy * hyy + hyz * hyz) + (hzx * hzx + hzy * hzy + hzz * hzz)
+    nu_mu = float((dissipte * lem[c3] * p.pra + dissipte2 * lec[c3] * p.pra).sum())
+    tx = (s.temp[kp] - t) * dxc[c3]
+    ty = (_jp(t) - t) * g.dy
+    tz = (_ip(t) - t) * g.dz
+    dissipth = tx * tx + ty * ty + tz * tz
+    nu_th = float((dissipth * lem[c3]).sum())
+    disste = ((dissipte + dissipte2) / (p.ren * float(nym) * float(nzm))).sum(axis=(1, 2))
+    dissth = (dissipth / (p.pec * float(nym) * float(nzm))).sum(axis=(1, 2))
+    volt = 1.0 / (float(nxm) * float(nzm) * float(nym))
+    return dict(nu_mu=nu_mu * volt + 1, nu_th=nu_th * volt, disste=disste, dissth=dissth)
+
+
+STAT_NAMES = ("vx_me", "vy_me", "vz_me", "temp_me", "vx_rms", "vy_rms", "vz_rms", "temp_rms",
+              "tempvx_me", "disste", "dissth")
+
+
+def calc_stats(s: State, acc: dict | None = None) -> dict:
+    """Horizontal means of CalcStats (StatRoutines.F90:21-43), added to the
+    accumulators ``acc`` (created zeroed on first use, with the sample count
+    ``nstatsamples``)."""
+    p = s.p
+    nxm = p.nxm
+    if acc is None:
+        acc = {k: np.zeros(nxm) for k in STAT_NAMES}
+        acc["nstatsamples"] = 0
+    acc["nstatsamples"] += 1
+    usnym, usnzm = 1.0 / p.nym, 1.0 / p.nzm
+    kc = slice(0, nxm)
+    vx, vy, vz, t = s.vx[kc], s.vy[kc], s.vz[kc], s.temp[kc]
+    for name, q in (("vx_me", vx), ("vy_me", vy), ("vz_me", vz), ("temp_me", t),
+                    ("vx_rms", vx ** 2), ("vy_rms", vy ** 2), ("vz_rms", vz ** 2),
+                    ("temp_rms", t ** 2), ("tempvx_me", t * vx)):
+        acc[name] += (q * usnzm * usnym).sum(axis=(1, 2))
+    return acc
+
+
+def slab_locations(g: Grid, nxm: int, xslab) -> list[int]:
+    """kslab(1..9) of InitializeSlabDump (SlabDumpRoutines.F90:52-67), 1-based:
+    slab m = 2..9 sits at the first k whose cell centre interval
+    (xm(k-1), xm(k)) contains xslab(m); kslab(1) = 2."""
+    kslab = [2] * 9
+    for k in range(2, nxm + 1):
+        for m in range(2, 10):
+            if g.xm[k - 1] > xslab[m - 2] and g.xm[k - 2] < xslab[m - 2]:
+                kslab[m - 1] = k
+    return kslab
+
+
+def slab_dump(s: State, kslab) -> np.ndarray:
+    """The four horizontal slabs of SlabDumper (SlabDumpRoutines.F90:15-24)
+    at each 1-based kslab: (vx(k) + vx(k+1)) / 2, vy(k), vz(k), temp(k).
+    Returns an array (len(kslab), 4, nym, nzm)."""
+    out = []
+    for k in kslab:
+        kk = k - 1
+        out.append(np.stack([(s.vx[kk] + s.vx[kk + 1]) * 0.5, s.vy[kk], s.vz[kk], s.temp[kk]]))
+    return np.array(out)
 
 
 def choose_dt(ntime: int, instcfl: float, dt: float, idtv: int, cflmax: float,
