@@ -8,8 +8,8 @@ kernel (afid_step_profiled), and keeps the fastest:
 * ky columns per z-FFT block (forward and inverse z transforms),
 * the variant of the explicit/forward kernel: 32x8-column tiles with 2
   resident blocks (up to 128 registers per thread), with 3 (up to 80), or
-  with two x-planes per barrier; 32x4 tiles with 4 blocks; 32x2 tiles with
-  8 blocks.
+  with two x-planes per barrier; 32x4 tiles with 4, 5 or 6 blocks; 32x2
+  tiles with 8 blocks.
 
 Results do not depend on the shapes (tests/test_gpu_batch.py checks batched
 against single-box results bit for bit), so tuning is purely a speed choice.
@@ -61,7 +61,7 @@ def candidates(cfg: BouIn) -> dict:
     ny = [v for v in (1, 2, 4, 8, 16) if fft_y_bytes(cfg.nym, v) <= SMEM_MAX and v * cfg.nym <= TILE_MAX]
     nz = [v for v in (1, 2, 4, 8, 16) if fft_z_bytes(cfg.nzm, v) <= SMEM_MAX and v * cfg.nzm <= TILE_MAX
           and v < 2 * (cfg.nym // 2 + 1)]
-    return {"fft_y_lines": ny or [1], "fft_z_lines": nz or [1], "k1_minb": [2, 3, 4, 5, 6]}
+    return {"fft_y_lines": ny or [1], "fft_z_lines": nz or [1], "k1_minb": [2, 3, 4, 5, 6, 7, 8]}
 
 
 def class_key(cfg: BouIn) -> str:

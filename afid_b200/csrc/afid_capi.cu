@@ -104,8 +104,9 @@ int factor_radices(int n, int *rad, int *np) {
 //   2: 32x8 tiles, 2 blocks/SM        3: 32x8 tiles, 3 blocks/SM (80 registers)
 //   4: 32x8 tiles, two planes per barrier
 //   5: 32x4 tiles, 4 blocks/SM        6: 32x2 tiles, 8 blocks/SM
-constexpr int K1_VMIN = 2, K1_VMAX = 6;
-int k1_tile_height(int variant) { return variant == 5 ? 4 : variant == 6 ? 2 : 8; }
+//   7: 32x4 tiles, 5 blocks/SM        8: 32x4 tiles, 6 blocks/SM
+constexpr int K1_VMIN = 2, K1_VMAX = 8;
+int k1_tile_height(int variant) { return (variant == 5 || variant >= 7) ? 4 : variant == 6 ? 2 : 8; }
 
 long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2) {
   switch (fam) {
@@ -376,6 +377,8 @@ int init_kernel_attrs() {
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<2, 8>::SMEM));
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<4, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 4>::SMEM));
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<2, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 2>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<4, 5, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 4>::SMEM));
+  CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<4, 6, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 4>::SMEM));
   const int fsm = FFT_SMEM_MAX;   // two slots + work + twiddles: (4 N + 4) 16 bytes at one line
   CK(cudaFuncSetAttribute(k_fft_y_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
@@ -445,6 +448,8 @@ int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) 
     case 4: k_explicit_implicit_fwd<8, 2, 2><<<nk1, 256, K1Ring<2, 8>::SMEM, s>>>(k1, ns); break;
     case 5: k_explicit_implicit_fwd<4, 4, 1><<<nk1, 128, K1Ring<1, 4>::SMEM, s>>>(k1, ns); break;
     case 6: k_explicit_implicit_fwd<2, 8, 1><<<nk1, 64, K1Ring<1, 2>::SMEM, s>>>(k1, ns); break;
+    case 7: k_explicit_implicit_fwd<4, 5, 1><<<nk1, 128, K1Ring<1, 4>::SMEM, s>>>(k1, ns); break;
+    case 8: k_explicit_implicit_fwd<4, 6, 1><<<nk1, 128, K1Ring<1, 4>::SMEM, s>>>(k1, ns); break;
     default: k_explicit_implicit_fwd<8, 2, 1><<<nk1, 256, K1Ring<1, 8>::SMEM, s>>>(k1, ns); break;
   }
   CKL();
@@ -823,6 +828,19 @@ int afid_box_reset(afid_ctx *c, int id, double dt) {
   if (dt > 0) bs.dt = dt;
   CK(cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st));
   CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
+int afid_box_set_time(afid_ctx *c, int id, double time) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync((char *)hb->dev.sc + offsetof(BoxScalars, time), &time, sizeof time,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 

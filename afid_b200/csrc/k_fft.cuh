@@ -181,15 +181,19 @@ __device__ __forceinline__ void pass_inplace(int N, int lgL, int Ns, int sgn, co
   const int lmask = (1 << lgL) - 1;
   const FastDiv dNs(Ns);
   double2 v[BPT][R];
-  // every slot loads (idle ones repeat the last butterfly of their line): a
-  // conditional load here would keep v out of registers across the barrier
-  // thread t takes butterflies j = t / L + b FFT_T / L of line l = t % L
+  // thread t takes butterflies j = t / L + b FFT_T / L of line l = t % L;
+  // idle slots hold zeros (v must be defined on every path to stay in
+  // registers across the barrier)
   const int l = threadIdx.x & lmask, j0 = threadIdx.x >> lgL, jstep = FFT_T >> lgL;
 #pragma unroll
   for (int b = 0; b < BPT; ++b) {
-    const int jc = min(j0 + b * jstep, NR - 1);
+    const int j = j0 + b * jstep;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[b][r] = src(l, jc + r * NR);
+    for (int r = 0; r < R; ++r) v[b][r] = make_double2(0.0, 0.0);
+    if (j < NR) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = src(l, j + r * NR);
+    }
   }
   __syncthreads();
 #pragma unroll
@@ -393,14 +397,15 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
 
 // ---------------------------------------------------------------------------
 // z transform in place on spec[k][kz][ky] for a tile of L consecutive ky.
-// Forward transforms divide by nym*nzm (SolvePressureCorrection.F90:105).
+// The division of the forward transform by nym*nzm
+// (SolvePressureCorrection.F90:105) is done by k_poisson_x as it reads each
+// value, in the same operation order.
 // ---------------------------------------------------------------------------
 struct ZDst {
-  double2 *spec; int nh, ky0; double norm; bool scale;
+  double2 *spec; int nh, ky0;
   __device__ __forceinline__ void operator()(int l, int n, double2 v) const {
     const int ky = ky0 + l;
     if (ky >= nh) return;
-    if (scale) { v.x = v.x / norm; v.y = v.y / norm; }
     spec[(long long)n * nh + ky] = v;
   }
 };
@@ -451,7 +456,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn
       double2 *cur = slot[it & 1];
       const int lgL = ilog2(L);
       fft_tile<true>(cur, N, lgL, B.fft_z_radix, B.fft_z_np, sgn, tws, SmemSrc{cur, lgL},
-                            ZDst{B.spec + (long long)k * N * nh, nh, ky0, (double)(B.nzm * B.nym), sgn < 0});
+                            ZDst{B.spec + (long long)k * N * nh, nh, ky0});
     }
     __syncthreads();
   }
@@ -462,9 +467,11 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn
 // thread per (ky, kz), marching k.  Row k of the normalised system is
 //   amph(k) x(k-1) + x(k) + apph(k) x(k+1) = dphc(k) s(k),
 //   s(k) = 1 / (acphk(k) - ak2(ky) - ak1(kz)).
-// Its coefficients are real, so the complex Thomas sweep is a real sweep
-// applied to both parts.  The (0,0) mode is singular (Neumann in x): its
-// last equation is dropped and its last unknown set to zero.
+// dphc arrives unnormalised from the forward z transform and is divided by
+// nym*nzm here, before the scaling by s(k).  Its coefficients are real, so
+// the complex Thomas sweep is a real sweep applied to both parts.  The (0,0)
+// mode is singular (Neumann in x): its last equation is dropped and its last
+// unknown set to zero.
 // ---------------------------------------------------------------------------
 constexpr int KP_U = 4;   // planes per prefetch chunk of the sweeps
 
@@ -487,6 +494,7 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
   double *__restrict__ dst = B.dstore + m;
   const long long st = nmode;
   const bool zero_mode = (ky == 0 && kz == 0);
+  const double norm = (double)(B.nzm * B.nym);   // the forward transforms' 1/(nym nzm)
   // forward elimination (dgttrf + dgttrs forward sweep), planes in chunks
   double d = 1.0, ap_prev = 0.0;
   double2 y = make_double2(0.0, 0.0);
@@ -501,6 +509,7 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
       if (k >= nxm) break;
       const double s = 1.0 / ((__ldg(acph + k) - ak) - ak1);
       double2 rk = r[u];
+      rk.x = rk.x / norm; rk.y = rk.y / norm;
       rk.x = rk.x * s; rk.y = rk.y * s;
       if (k == 0) {
         y = rk;

@@ -178,6 +178,10 @@ class Box:
         _lib.check(self._L.afid_box_set_tuning(self.ctx.h, self.id, fft_y_lines, fft_z_lines, k1_minb))
         self.tuning = (fft_y_lines, fft_z_lines, k1_minb)
 
+    def set_time(self, time: float):
+        """Simulation time of the box (as restored from continua files)."""
+        _lib.check(self._L.afid_box_set_time(self.ctx.h, self.id, float(time)))
+
     def reset(self, dt: float = 0.0):
         _lib.check(self._L.afid_box_reset(self.ctx.h, self.id, dt))
 

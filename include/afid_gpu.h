@@ -124,14 +124,17 @@ int afid_box_download(afid_ctx *ctx, int box_id, int field, double *host);
 /* Zero the RK history, the carried rhs wall row, time, step count and
  * status; set dt (values <= 0 keep the current dt). */
 int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
+/* Set the simulation time (the time a restart reads from the continua
+ * master record, ReadFlowField.F90:24-40). */
+int afid_box_set_time(afid_ctx *ctx, int box_id, double time);
 int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
 /* Launch-shape tuning of one box (no counterpart in the reference):
  * row pairs per y-FFT block and ky columns per z-FFT block (powers of two;
  * 0 = built-in choice) and the variant of the explicit/forward kernel:
  * 2 = 32x8-column tiles, two resident blocks per SM; 3 = 32x8, three
- * resident blocks; 4 = 32x8, two planes per barrier; 5 = 32x4 tiles, four
- * blocks; 6 = 32x2 tiles, eight blocks (0 = 2).  Results do not depend on
- * these values. */
+ * resident blocks; 4 = 32x8, two planes per barrier; 5, 7, 8 = 32x4 tiles,
+ * four, five or six blocks; 6 = 32x2 tiles, eight blocks (0 = 2).  Results
+ * do not depend on these values. */
 int afid_box_set_tuning(afid_ctx *ctx, int box_id, int fft_y_lines, int fft_z_lines, int k1_minb);
 /* Copies up to max_records of the most recent per-step records, oldest
  * first; returns the number copied (>= 0) or an error code. */

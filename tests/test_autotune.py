@@ -31,7 +31,7 @@ def test_candidates_fit_shared_memory(nyz):
         assert (2 * v * nyz + nyz) * 16 <= 200 * 1024 and v * nyz <= 14 * 256
         assert v & (v - 1) == 0
     assert c["fft_y_lines"] and c["fft_z_lines"]
-    assert c["k1_minb"] == [2, 3, 4, 5, 6]
+    assert c["k1_minb"] == [2, 3, 4, 5, 6, 7, 8]
 
 
 def test_cache_roundtrip(tmp_path):

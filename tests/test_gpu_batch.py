@@ -94,7 +94,7 @@ def test_fft_size_rule(ctx):
         ctx.add_box(cfg_of(16, 22, 16))
 
 
-@pytest.mark.parametrize("fy,fz,k1", [(1, 2, 3), (2, 1, 4), (4, 4, 5), (2, 8, 6)])
+@pytest.mark.parametrize("fy,fz,k1", [(1, 2, 3), (2, 1, 4), (4, 4, 5), (2, 8, 6), (1, 4, 7), (8, 2, 8)])
 def test_launch_shapes_do_not_change_results(ctx, fy, fz, k1):
     """Tuned launch shapes (FFT lines per block, tile shape and occupancy of
     the explicit kernel) give bit-identical fields."""
@@ -106,7 +106,7 @@ def test_launch_shapes_do_not_change_results(ctx, fy, fz, k1):
     for f in FIELDS:
         assert np.array_equal(a.download(f), b.download(f)), f
     from afid_b200._lib import AfidError
-    for bad in (dict(fft_y_lines=10 ** 6), dict(fft_y_lines=3), dict(fft_z_lines=6), dict(k1_minb=7)):
+    for bad in (dict(fft_y_lines=10 ** 6), dict(fft_y_lines=3), dict(fft_z_lines=6), dict(k1_minb=9)):
         with pytest.raises(AfidError):
             b.set_tuning(**bad)
     for x in (a, b):
