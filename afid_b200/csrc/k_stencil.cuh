@@ -675,7 +675,7 @@ __device__ __forceinline__ double local_div(const BoxDev &B, int k, int j, int i
 // Column march: one thread per (j, i), planes in chunks whose loads are all
 // in flight together; vx(k+1) of one plane is vx(k) of the next.
 constexpr int KD_U = 4;
-__global__ void __launch_bounds__(256, 3) k_divergence(BatchDev bt, int ns) {
+__global__ void __launch_bounds__(256, 2) k_divergence(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
