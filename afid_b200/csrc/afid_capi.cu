@@ -353,7 +353,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   {
     int rc = init_kernel_attrs();
     if (!rc) rc = fft_grid(k_fft_y_fwd, bt->smem_y, bt->total[FAM_FY], &bt->grid_y);
-    if (!rc) rc = fft_grid(k_fft_z, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
+    if (!rc) rc = fft_grid(k_fft_z<-1>, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
     if (rc) { free_batch(bt); return rc; }
   }
   c->batches[key] = bt;
@@ -382,7 +382,8 @@ int init_kernel_attrs() {
   const int fsm = FFT_SMEM_MAX;   // two slots + work + twiddles: (4 N + 4) 16 bytes at one line
   CK(cudaFuncSetAttribute(k_fft_y_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  CK(cudaFuncSetAttribute(k_fft_z, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fft_z<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fft_z<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   done = true;
   return 0;
 }
@@ -421,13 +422,13 @@ int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof 
   k_fft_y_fwd<<<bt->grid_y, FFT_T, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns, bt->sm_y, bt->total[FAM_FY]);
   CKL();
   PMARK(pf, AFID_K_FFT_Y_FWD);
-  k_fft_z<<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, -1, bt->sm_z, bt->total[FAM_FZ]);
+  k_fft_z<-1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
   PMARK(pf, AFID_K_FFT_Z_FWD);
   k_poisson_x<<<bt->total[FAM_PX], 256, 0, s>>>(bdev(bt, FAM_PX), ns);
   CKL();
   PMARK(pf, AFID_K_POISSON_X);
-  k_fft_z<<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, +1, bt->sm_z, bt->total[FAM_FZ]);
+  k_fft_z<+1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
   PMARK(pf, AFID_K_FFT_Z_INV);
   k_fft_y_inv<<<bt->grid_y, FFT_T, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns, bt->sm_y, bt->total[FAM_FY]);
@@ -1504,15 +1505,15 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   const size_t sy = (size_t)(2 * smy.slot + twy) * 16;
   const size_t sz = (size_t)(2 * smz.slot + twz) * 16;
   rc = fft_grid(k_fft_y_fwd, sy, off[0][1], &gy);
-  if (!rc) rc = fft_grid(k_fft_z, sz, off[1][1], &gz);
+  if (!rc) rc = fft_grid(k_fft_z<-1>, sz, off[1][1], &gz);
   if (rc) return rc;
   k_fft_y_fwd<<<gy, FFT_T, sy, st>>>(fy, 0, smy, off[0][1]);
   CKL();
-  k_fft_z<<<gz, FFT_T, sz, st>>>(fz, 0, -1, smz, off[1][1]);
+  k_fft_z<-1><<<gz, FFT_T, sz, st>>>(fz, 0, smz, off[1][1]);
   CKL();
   k_poisson_x<<<off[2][1], 256, 0, st>>>(px, 0);
   CKL();
-  k_fft_z<<<gz, FFT_T, sz, st>>>(fz, 0, +1, smz, off[1][1]);
+  k_fft_z<+1><<<gz, FFT_T, sz, st>>>(fz, 0, smz, off[1][1]);
   CKL();
   k_fft_y_inv<<<gy, FFT_T, sy, st>>>(fy, 0, smy, off[0][1]);
   CKL();

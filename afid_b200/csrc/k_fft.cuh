@@ -17,27 +17,32 @@
 
 namespace afid {
 
-// radix-R butterfly on v[0..R-1] (unnormalised DFT, exponent sign ``sgn``)
-__device__ __forceinline__ double2 cmul_wi(double2 a, double c, double s, int sgn) {
-  // a * (c + i sgn s)
-  const double ss = sgn > 0 ? s : -s;
+// Butterflies of the unnormalised DFT with exponent sign SGN (-1 forward,
+// +1 inverse), a compile-time constant so that every multiplication by +-i
+// and every conjugation is a sign flip.
+template <int SGN>
+__device__ __forceinline__ double2 cmul_wi(double2 a, double c, double s) {
+  // a * (c + i SGN s)
+  const double ss = SGN > 0 ? s : -s;
   return make_double2(a.x * c - a.y * ss, a.x * ss + a.y * c);
 }
-__device__ __forceinline__ double2 mul_sgn_i(double2 a, int sgn) {   // a * (sgn i)
-  return make_double2(-sgn * a.y, sgn * a.x);
+template <int SGN>
+__device__ __forceinline__ double2 mul_sgn_i(double2 a) {   // a * (SGN i)
+  return SGN > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
 }
-__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, double2 &a3, int sgn) {
+template <int SGN>
+__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, double2 &a3) {
   const double2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
   const double2 t2 = cadd(a1, a3), t3 = csub(a1, a3);
-  const double2 wt3 = mul_sgn_i(t3, sgn);
+  const double2 wt3 = mul_sgn_i<SGN>(t3);
   a0 = cadd(t0, t2);
   a2 = csub(t0, t2);
   a1 = cadd(t1, wt3);
   a3 = csub(t1, wt3);
 }
 
-template <int R>
-__device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double2 *tw, int N) {
+template <int R, int SGN>
+__device__ __forceinline__ void dft_small(double2 (&v)[R], const double2 *tw, int N) {
   constexpr double H = 0.70710678118654752440;    // cos(pi/4)
   constexpr double C8 = 0.92387953251128675613;   // cos(pi/8)
   constexpr double S8 = 0.38268343236508977173;   // sin(pi/8)
@@ -46,17 +51,17 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   } else if constexpr (R == 4) {
-    dft4(v[0], v[1], v[2], v[3], sgn);
+    dft4<SGN>(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 8) {
     // 8 = 2 x 4: four-point DFTs over n2 of x[n1 + 2 n2], twiddle W8^(n1 k2),
     // two-point DFTs over n1; X[4 k1 + k2]
     double2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
     double2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
-    dft4(a0, a1, a2, a3, sgn);
-    dft4(b0, b1, b2, b3, sgn);
-    b1 = cmul_wi(b1, H, H, sgn);
-    b2 = mul_sgn_i(b2, sgn);
-    b3 = cmul_wi(b3, -H, H, sgn);
+    dft4<SGN>(a0, a1, a2, a3);
+    dft4<SGN>(b0, b1, b2, b3);
+    b1 = cmul_wi<SGN>(b1, H, H);
+    b2 = mul_sgn_i<SGN>(b2);
+    b3 = cmul_wi<SGN>(b3, -H, H);
     v[0] = cadd(a0, b0); v[4] = csub(a0, b0);
     v[1] = cadd(a1, b1); v[5] = csub(a1, b1);
     v[2] = cadd(a2, b2); v[6] = csub(a2, b2);
@@ -67,18 +72,18 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
     // (X[4 k1 + k2] lands in v[4 k2 + k1]), then a register renaming into
     // natural order.
 #pragma unroll
-    for (int n1 = 0; n1 < 4; ++n1) dft4(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12], sgn);
-    v[5] = cmul_wi(v[5], C8, S8, sgn);        // n1=1 k2=1: m=1
-    v[9] = cmul_wi(v[9], H, H, sgn);          // n1=1 k2=2: m=2
-    v[13] = cmul_wi(v[13], S8, C8, sgn);      // n1=1 k2=3: m=3
-    v[6] = cmul_wi(v[6], H, H, sgn);          // n1=2 k2=1: m=2
-    v[10] = mul_sgn_i(v[10], sgn);            // n1=2 k2=2: m=4
-    v[14] = cmul_wi(v[14], -H, H, sgn);       // n1=2 k2=3: m=6
-    v[7] = cmul_wi(v[7], S8, C8, sgn);        // n1=3 k2=1: m=3
-    v[11] = cmul_wi(v[11], -H, H, sgn);       // n1=3 k2=2: m=6
-    v[15] = cmul_wi(v[15], -C8, -S8, sgn);    // n1=3 k2=3: m=9
+    for (int n1 = 0; n1 < 4; ++n1) dft4<SGN>(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+    v[5] = cmul_wi<SGN>(v[5], C8, S8);        // n1=1 k2=1: m=1
+    v[9] = cmul_wi<SGN>(v[9], H, H);          // n1=1 k2=2: m=2
+    v[13] = cmul_wi<SGN>(v[13], S8, C8);      // n1=1 k2=3: m=3
+    v[6] = cmul_wi<SGN>(v[6], H, H);          // n1=2 k2=1: m=2
+    v[10] = mul_sgn_i<SGN>(v[10]);            // n1=2 k2=2: m=4
+    v[14] = cmul_wi<SGN>(v[14], -H, H);       // n1=2 k2=3: m=6
+    v[7] = cmul_wi<SGN>(v[7], S8, C8);        // n1=3 k2=1: m=3
+    v[11] = cmul_wi<SGN>(v[11], -H, H);       // n1=3 k2=2: m=6
+    v[15] = cmul_wi<SGN>(v[15], -C8, -S8);    // n1=3 k2=3: m=9
 #pragma unroll
-    for (int k2 = 0; k2 < 4; ++k2) dft4(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3], sgn);
+    for (int k2 = 0; k2 < 4; ++k2) dft4<SGN>(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3]);
     // X[4 k1 + k2] = v[4 k2 + k1]: transpose the 4 x 4 index grid
     double2 t;
     t = v[1]; v[1] = v[4]; v[4] = t;
@@ -92,7 +97,7 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
     const double2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
     const double2 a0 = v[0];
     const double2 m = make_double2(a0.x - 0.5 * s.x, a0.y - 0.5 * s.y);
-    const double2 id = make_double2(-sgn * S3 * d.y, sgn * S3 * d.x);
+    const double2 id = make_double2((-SGN * S3) * d.y, (SGN * S3) * d.x);
     v[0] = cadd(a0, s);
     v[1] = cadd(m, id);
     v[2] = csub(m, id);
@@ -106,8 +111,8 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
     const double2 r2 = make_double2(a0.x + C2 * s14.x + C1 * s23.x, a0.y + C2 * s14.y + C1 * s23.y);
     const double2 q1 = make_double2(S1 * d14.x + S2 * d23.x, S1 * d14.y + S2 * d23.y);
     const double2 q2 = make_double2(S2 * d14.x - S1 * d23.x, S2 * d14.y - S1 * d23.y);
-    const double2 iq1 = mul_sgn_i(q1, sgn);
-    const double2 iq2 = mul_sgn_i(q2, sgn);
+    const double2 iq1 = mul_sgn_i<SGN>(q1);
+    const double2 iq2 = mul_sgn_i<SGN>(q2);
     v[0] = make_double2(a0.x + s14.x + s23.x, a0.y + s14.y + s23.y);
     v[1] = cadd(r1, iq1);
     v[4] = csub(r1, iq1);
@@ -123,7 +128,7 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], int sgn, const double
 #pragma unroll
       for (int m = 1; m < R; ++m) {
         double2 w = tw[((m * q) % R) * step];
-        if (sgn > 0) w.y = -w.y;
+        if (SGN > 0) w.y = -w.y;
         acc = cadd(acc, cmul(v[m], w));
       }
       out[q] = acc;
@@ -160,12 +165,12 @@ struct FastDiv {
   __device__ __forceinline__ int mod(int n) const { return p2 ? (n & (d - 1)) : n % d; }
 };
 
-template <int R>
-__device__ __forceinline__ void twiddle(double2 (&v)[R], int k, int tstr, int sgn, const double2 *tw) {
+template <int R, int SGN>
+__device__ __forceinline__ void twiddle(double2 (&v)[R], int k, int tstr, const double2 *tw) {
 #pragma unroll
   for (int r = 1; r < R; ++r) {
     double2 w = tw[r * k * tstr];
-    if (sgn > 0) w.y = -w.y;
+    if (SGN > 0) w.y = -w.y;
     v[r] = cmul(v[r], w);
   }
 }
@@ -173,8 +178,8 @@ __device__ __forceinline__ void twiddle(double2 (&v)[R], int k, int tstr, int sg
 // element (l, n) of a tile of L lines (L a power of two) at n*L + l
 __device__ __forceinline__ int sidx(int l, int n, int lgL) { return (n << lgL) + l; }
 
-template <int R, class Src, class Dst>
-__device__ __forceinline__ void pass_inplace(int N, int lgL, int Ns, int sgn, const double2 *tw,
+template <int R, int SGN, class Src, class Dst>
+__device__ __forceinline__ void pass_inplace(int N, int lgL, int Ns, const double2 *tw,
                                              const Src &src, const Dst &dst) {
   constexpr int BPT = 16 / R;               // butterflies per thread
   const int NR = N / R, tstr = N / (Ns * R);
@@ -201,8 +206,8 @@ __device__ __forceinline__ void pass_inplace(int N, int lgL, int Ns, int sgn, co
     const int j = j0 + b * jstep;
     if (j < NR) {
       const int k = dNs.mod(j);
-      if (Ns > 1) twiddle<R>(v[b], k, tstr, sgn, tw);
-      dft_small<R>(v[b], sgn, tw, N);
+      if (Ns > 1) twiddle<R, SGN>(v[b], k, tstr, tw);
+      dft_small<R, SGN>(v[b], tw, N);
       const int base = (j - k) * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) dst(l, base + r * Ns, v[b][r]);
@@ -211,17 +216,17 @@ __device__ __forceinline__ void pass_inplace(int N, int lgL, int Ns, int sgn, co
   __syncthreads();
 }
 
-template <class Src, class Dst>
-__device__ __forceinline__ void run_inplace(int R, int N, int lgL, int Ns, int sgn, const double2 *tw,
+template <int SGN, class Src, class Dst>
+__device__ __forceinline__ void run_inplace(int R, int N, int lgL, int Ns, const double2 *tw,
                                             const Src &src, const Dst &dst) {
   switch (R) {
-    case 16: pass_inplace<16>(N, lgL, Ns, sgn, tw, src, dst); break;
-    case 8: pass_inplace<8>(N, lgL, Ns, sgn, tw, src, dst); break;
-    case 4: pass_inplace<4>(N, lgL, Ns, sgn, tw, src, dst); break;
-    case 2: pass_inplace<2>(N, lgL, Ns, sgn, tw, src, dst); break;
-    case 3: pass_inplace<3>(N, lgL, Ns, sgn, tw, src, dst); break;
-    case 5: pass_inplace<5>(N, lgL, Ns, sgn, tw, src, dst); break;
-    default: pass_inplace<7>(N, lgL, Ns, sgn, tw, src, dst); break;
+    case 16: pass_inplace<16, SGN>(N, lgL, Ns, tw, src, dst); break;
+    case 8: pass_inplace<8, SGN>(N, lgL, Ns, tw, src, dst); break;
+    case 4: pass_inplace<4, SGN>(N, lgL, Ns, tw, src, dst); break;
+    case 2: pass_inplace<2, SGN>(N, lgL, Ns, tw, src, dst); break;
+    case 3: pass_inplace<3, SGN>(N, lgL, Ns, tw, src, dst); break;
+    case 5: pass_inplace<5, SGN>(N, lgL, Ns, tw, src, dst); break;
+    default: pass_inplace<7, SGN>(N, lgL, Ns, tw, src, dst); break;
   }
 }
 
@@ -237,24 +242,24 @@ struct SmemSrc {
 // Whole transform of a tile held in shared buffer a: the first pass reads
 // ``src``, the last pass writes ``dst`` when LAST_TO_DST (otherwise the
 // result stays in a).
-template <bool LAST_TO_DST, class Src, class Dst>
-__device__ void fft_tile(double2 *a, int N, int lgL, const int *rad, int np, int sgn, const double2 *tw,
+template <bool LAST_TO_DST, int SGN, class Src, class Dst>
+__device__ void fft_tile(double2 *a, int N, int lgL, const int *rad, int np, const double2 *tw,
                          const Src &src, const Dst &dst) {
   const SmemSrc as{a, lgL};
   const SmemDst ad{a, lgL};
   if (np == 1) {
-    if (LAST_TO_DST) run_inplace(rad[0], N, lgL, 1, sgn, tw, src, dst);
-    else run_inplace(rad[0], N, lgL, 1, sgn, tw, src, ad);
+    if (LAST_TO_DST) run_inplace<SGN>(rad[0], N, lgL, 1, tw, src, dst);
+    else run_inplace<SGN>(rad[0], N, lgL, 1, tw, src, ad);
     return;
   }
-  run_inplace(rad[0], N, lgL, 1, sgn, tw, src, ad);
+  run_inplace<SGN>(rad[0], N, lgL, 1, tw, src, ad);
   int Ns = rad[0];
   for (int p = 1; p < np - 1; ++p) {
-    run_inplace(rad[p], N, lgL, Ns, sgn, tw, as, ad);
+    run_inplace<SGN>(rad[p], N, lgL, Ns, tw, as, ad);
     Ns *= rad[p];
   }
-  if (LAST_TO_DST) run_inplace(rad[np - 1], N, lgL, Ns, sgn, tw, as, dst);
-  else run_inplace(rad[np - 1], N, lgL, Ns, sgn, tw, as, ad);
+  if (LAST_TO_DST) run_inplace<SGN>(rad[np - 1], N, lgL, Ns, tw, as, dst);
+  else run_inplace<SGN>(rad[np - 1], N, lgL, Ns, tw, as, ad);
 }
 
 // Persistent transform blocks.  A launch has at most (SMs x resident blocks)
@@ -374,7 +379,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
       const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
       double2 *cur = slot[it & 1];
       const int lgP = ilog2(Pp);
-      fft_tile<false>(cur, N, lgP, B.fft_y_radix, B.fft_y_np, -1, tws, PairSrc{(const double *)cur, N + 1},
+      fft_tile<false, -1>(cur, N, lgP, B.fft_y_radix, B.fft_y_np, tws, PairSrc{(const double *)cur, N + 1},
                       NoDst{});
       // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
       // B = (Z_q - conj Z_{N-q}) / (2i)
@@ -422,7 +427,8 @@ __device__ __forceinline__ void fft_z_copy_in(const BoxDev &B, int lt, double2 *
   }
 }
 
-__global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn, FftSmem sm, int total) {
+template <int SGN>
+__global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem sm, int total) {
   extern __shared__ double2 fsm[];
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
@@ -455,7 +461,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, int sgn
       const int k = lt / ntl, ky0 = (lt - k * ntl) * L;
       double2 *cur = slot[it & 1];
       const int lgL = ilog2(L);
-      fft_tile<true>(cur, N, lgL, B.fft_z_radix, B.fft_z_np, sgn, tws, SmemSrc{cur, lgL},
+      fft_tile<true, SGN>(cur, N, lgL, B.fft_z_radix, B.fft_z_np, tws, SmemSrc{cur, lgL},
                             ZDst{B.spec + (long long)k * N * nh, nh, ky0});
     }
     __syncthreads();
@@ -627,7 +633,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, Fft
       const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
       const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
       double2 *cur = slot[it & 1];
-      fft_tile<true>(cur, N, ilog2(Pp), B.fft_y_radix, B.fft_y_np, +1, tws, YInvSmemSrc{cur, N, nh, (N % 2) == 0},
+      fft_tile<true, +1>(cur, N, ilog2(Pp), B.fft_y_radix, B.fft_y_np, tws, YInvSmemSrc{cur, N, nh, (N % 2) == 0},
                            YInvDst{B.phi + (long long)k * B.plane, N, nzm, i0});
     }
     __syncthreads();
