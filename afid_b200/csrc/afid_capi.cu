@@ -70,7 +70,7 @@ struct Batch {
   int *d_off = nullptr;     // NFAM x (nbox + 1)
   int total[NFAM] = {};
   size_t smem_y = 0, smem_z = 0;
-  FftSmem sm_y{0}, sm_z{0};         // slot sizes of the persistent transforms
+  FftSmem sm_y{0, 0}, sm_z{0, 0};   // slot and twiddle sizes of the persistent transforms
   int grid_y = 0, grid_z = 0;       // their resident grids
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
@@ -136,7 +136,8 @@ Sizes sizes_of(const afid_box_params &p) {
   // tables + twiddles + coef + nu partials + history + scalars (in doubles)
   s.small = (long long)T_NK * s.nx + p.nzm + p.nym + 2LL * (p.nym + p.nzm) +
             (long long)SYS_N * C_N * s.nx + 2 * NU_BLOCKS + (long long)HIST_CAP * HIST_FIELDS +
-            (long long)(sizeof(BoxScalars) / 8 + 8) + s.plane;
+            (long long)(sizeof(BoxScalars) / 8 + 8) + s.plane +
+            64;   // alignment of the scalars and the 128-byte TMA map (64-byte aligned)
   return s;
 }
 
@@ -243,6 +244,60 @@ void build_twiddles(int n, double2 *w) {
   }
 }
 
+
+// ---- TMA maps -----------------------------------------------------------------
+// cuTensorMapEncodeTiled is a driver entry point; it is looked up through the
+// runtime so that the library needs no link-time dependency on libcuda.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// largest divisor of n not above 256 (kz rows per TMA box)
+int tma_rows(int n) {
+  for (int r = n < 256 ? n : 256; r > 1; --r)
+    if (n % r == 0) return r;
+  return 1;
+}
+
+// encode the z-transform map of box d (its spec array, box 2L x rb doubles)
+int encode_z_map(BoxDev &d, CUtensorMap *out) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return fail(AFID_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const int L = fft_z_lines(d);
+  d.fz_rb = tma_rows(d.nzm);
+  const cuuint64_t dims[2] = {(cuuint64_t)2 * d.nymh, (cuuint64_t)d.nxm * d.nzm};
+  const cuuint64_t strides[1] = {(cuuint64_t)2 * d.nymh * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * L), (cuuint32_t)d.fz_rb};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)d.spec, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(AFID_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return 0;
+}
+
+// encode box d's z map and copy it to its device slot d.tm_z
+int write_z_map(BoxDev &d, cudaStream_t st) {
+  CUtensorMap m;
+  int rc = encode_z_map(d, &m);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync((void *)d.tm_z, &m, sizeof m, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}
+
 }  // namespace
 
 struct afid_ctx {
@@ -285,6 +340,8 @@ void fft_smem_grow(const BoxDev &d, FftSmem &y, FftSmem &z, int &twy, int &twz) 
   const int Pp = fft_y_pairs(d), L = fft_z_lines(d);
   y.slot = std::max(y.slot, fft_y_slot(d.nym, Pp));
   z.slot = std::max(z.slot, L * d.nzm);
+  y.tw = std::max(y.tw, d.nym);
+  z.tw = std::max(z.tw, d.nzm);
   twy = std::max(twy, d.nym);
   twz = std::max(twz, d.nzm);
 }
@@ -321,7 +378,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     fft_smem_grow(d, bt->sm_y, bt->sm_z, twy_max, twz_max);
   }
   bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16;
-  bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16;
+  bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16 + 16;   // + two mbarriers
   {
     // one variant of the explicit/forward kernel per launch: the one the
     // boxes holding most of the cells ask for
@@ -707,7 +764,14 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   d.hist = M + o; o += (size_t)HIST_CAP * HIST_FIELDS;
   d.wall = M + o; o += (size_t)s.plane;
   o = (o + 7) & ~(size_t)7;
-  d.sc = (BoxScalars *)(M + o);
+  d.sc = (BoxScalars *)(M + o); o += (sizeof(BoxScalars) + 63) / 8;
+  o = (o + 7) & ~(size_t)7;   // 64-byte aligned (mem_small is 256-byte aligned)
+  d.tm_z = (const CUtensorMap *)(M + o); o += sizeof(CUtensorMap) / 8;
+  if ((long long)o > s.small) {
+    cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small); cudaFree(hb->d_self);
+    delete hb;
+    return fail(AFID_ECUDA, "box_add: small-region layout exceeds its allocation");
+  }
   std::vector<double2> tw((size_t)p->nym + p->nzm);
   build_twiddles(p->nym, tw.data());
   build_twiddles(p->nzm, tw.data() + p->nym);
@@ -727,6 +791,12 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
     cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small); cudaFree(hb->d_self);
     delete hb;
     return fail(AFID_ECUDA, "box_add: initialisation copy failed");
+  }
+  rc = write_z_map(hb->dev, st);
+  if (rc) {
+    cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small); cudaFree(hb->d_self);
+    delete hb;
+    return rc;
   }
   hb->id = c->next_id++;
   hb->xc.assign(xc, xc + p->nxm + 1);
@@ -903,6 +973,8 @@ int afid_box_set_tuning(afid_ctx *c, int id, int fft_y_lines, int fft_z_lines, i
   d.fy_lines = fft_y_lines;
   d.fz_lines = fft_z_lines;
   d.k1_minb = k1_minb ? k1_minb : 2;
+  rc = write_z_map(d, c->stream);   // the TMA box width follows the z lines
+  if (rc) return rc;
   // batches hold copies of the descriptor and tile tables: drop them
   for (auto it = c->batches.begin(); it != c->batches.end();) {
     bool has = false;
@@ -1388,6 +1460,7 @@ int noalloc_setup(int dev) {
 struct NoallocHost {
   double tab[(size_t)T_NK * (NOALLOC_MAX_NXM + 1) + 2 * NOALLOC_MAX_NYZ];
   double2 tw[2 * NOALLOC_MAX_NYZ];
+  CUtensorMap tm;
 };
 NoallocHost g_noalloc_host;
 
@@ -1430,7 +1503,8 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   const long long o_sc = (o_tw + 2LL * (nym + nzm) + 7) & ~7LL;
   const long long o_box = o_sc + (long long)((sizeof(BoxScalars) + 63) / 8);
   const long long o_off = o_box + (long long)((sizeof(BoxDev) + 63) / 8);
-  if (o_off + 16 > AFID_NOALLOC_DOUBLES) return fail(AFID_ESIZE, "noalloc: tables do not fit");
+  const long long o_tm = (o_off + 16 + 7) & ~7LL;   // 64-byte aligned TMA map of the z transform
+  if (o_tm + 16 > AFID_NOALLOC_DOUBLES) return fail(AFID_ESIZE, "noalloc: tables do not fit");
 
   // tables: the Poisson rows of InitPressureSolver.F90:22-59 (other k-tables unused)
   double *tab = g_noalloc_host.tab;
@@ -1484,7 +1558,10 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   d.twy = (const double2 *)(base + o_tw);
   d.twz = (const double2 *)(base + o_tw) + nym;
   d.sc = (BoxScalars *)(base + o_sc);
+  d.tm_z = (const CUtensorMap *)(base + o_tm);
   d.active = 1;
+  rc = encode_z_map(d, &g_noalloc_host.tm);
+  if (rc) return rc;
   BoxScalars bs;
   memset(&bs, 0, sizeof bs);
   int off[3][2];
@@ -1496,14 +1573,15 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   CK(cudaMemcpyAsync(base + o_sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_box, &d, sizeof d, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_off, off, sizeof off, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + o_tm, &g_noalloc_host.tm, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
   const BoxDev *dbox = (const BoxDev *)(base + o_box);
   const int *doff = (const int *)(base + o_off);
   BatchDev fy{dbox, doff + 0, 1}, fz{dbox, doff + 2, 1}, px{dbox, doff + 4, 1};
-  FftSmem smy{0}, smz{0};
+  FftSmem smy{0, 0}, smz{0, 0};
   int twy = 0, twz = 0, gy = 0, gz = 0;
   fft_smem_grow(d, smy, smz, twy, twz);
   const size_t sy = (size_t)(2 * smy.slot + twy) * 16;
-  const size_t sz = (size_t)(2 * smz.slot + twz) * 16;
+  const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + 16;
   rc = fft_grid(k_fft_y_fwd, sy, off[0][1], &gy);
   if (!rc) rc = fft_grid(k_fft_z<-1>, sz, off[1][1], &gz);
   if (rc) return rc;

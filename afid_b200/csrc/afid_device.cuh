@@ -11,6 +11,7 @@
 //     keep the x-neighbours of their own column in a ring of planes.
 // There is no halo storage: periodic neighbours are index wraps.
 #pragma once
+#include <cuda.h>            // CUtensorMap
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -95,6 +96,8 @@ struct BoxDev {
   int k1_minb;          // tuning: variant of the explicit/forward kernel (2, 3 or 4)
   int fy_lines;         // tuning: row pairs per y-FFT block (0 = default)
   int fz_lines;         // tuning: ky columns per z-FFT block (0 = default)
+  int fz_rb;            // kz rows per TMA box of the z transform (a divisor of nzm, <= 256)
+  const CUtensorMap *tm_z;  // TMA map of spec as a 2-D FP64 array (2*nymh x nxm*nzm), box 2L x fz_rb
   int pad2_;
 };
 
@@ -155,6 +158,55 @@ __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_
 __device__ __forceinline__ void cp_async_commit_wait() {
   cp_async_commit();
   cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+// TMA (cp.async.bulk.tensor) loads into shared memory, completed on an
+// mbarrier.  Waits are bounded: after MBAR_MAX_TRIES polls the caller treats
+// the copy as failed (status AFID_STATUS_DEVICE_TIMEOUT) instead of spinning.
+// ---------------------------------------------------------------------------
+constexpr unsigned MBAR_MAX_TRIES = 1u << 22;
+constexpr int AFID_STATUS_DEVICE_TIMEOUT = 990;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// order this thread's generic-proxy shared-memory accesses before later
+// async-proxy (TMA) accesses
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
+  for (unsigned t = 0; t < MBAR_MAX_TRIES; ++t)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// 2-D tile load of box (x, y) of ``map`` into shared memory at dst (16-byte
+// aligned); x times the element size must be a multiple of 16 bytes
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x,
+                                            int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+      "[%2];\n" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
 }
 
 }  // namespace afid

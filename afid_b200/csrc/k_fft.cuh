@@ -1,6 +1,7 @@
 // Pressure Poisson solve of SolvePressureCorrection.F90:35-151 on one GPU:
 //   y: real-to-complex FFT (two real rows packed in one complex line) of dph;
-//   z: complex FFT along kz on tiles of consecutive ky (in place);
+//   z: complex FFT along kz on tiles of consecutive ky (in place), the tiles
+//      brought in by TMA;
 //   x: one complex tridiagonal per (ky, kz), Thomas in dgttrf/dgttrs order;
 //   then the inverse z and y transforms, the latter writing dph.
 // The 2DECOMP pencil transposes of the reference disappear: each transform
@@ -277,7 +278,7 @@ constexpr int FFT_MAX_LINES = 16;
 // 2 Pp half-spectrum rows of an inverse tile (2 Pp (N/2+1) complex)
 __host__ __device__ __forceinline__ int fft_y_slot(int N, int Pp) { return 2 * Pp * (N / 2 + 1); }  // >= Pp (N + 1)
 __host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 * fft_y_slot(N, Pp) + N) * 16; }
-__host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16; }
+__host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16 + 16; }
 __host__ __device__ __forceinline__ bool fft_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
 __host__ __device__ __forceinline__ bool fft_y_ok(int N, int Pp, int budget) {
   return fft_pow2(Pp) && Pp * N <= FFT_TILE_MAX && fft_y_bytes(N, Pp) <= budget;
@@ -308,6 +309,7 @@ __host__ __device__ __forceinline__ int fft_z_lines(const BoxDev &B) {
 // shared-memory layout of one launch (largest box of the batch)
 struct FftSmem {
   int slot;   // complex values per copy-in slot (the twiddles follow the two slots)
+  int tw;     // complex values of the twiddle table (the z transform's mbarriers follow it)
 };
 
 __device__ __forceinline__ int tile_box(const BatchDev &bt, int tile, int &local) {
@@ -415,16 +417,18 @@ struct ZDst {
   }
 };
 
-__device__ __forceinline__ void fft_z_copy_in(const BoxDev &B, int lt, double2 *a) {
-  const int N = B.nzm, nh = B.nymh, L = fft_z_lines(B);
+// The tile of L consecutive ky at all kz of plane k is a dense box of spec
+// seen as a 2-D FP64 array (2 nymh doubles per kz row, nxm nzm rows): one
+// thread loads it with nzm / fz_rb TMA copies of 2L x fz_rb doubles, which
+// land in shared memory as element (l, kz) at kz L + l; ky beyond nymh reads
+// as zero.  The copy of the next tile runs while the current one is
+// transformed; each slot completes on its own mbarrier.
+__device__ __forceinline__ void fft_z_issue(const BoxDev &B, int lt, double2 *a, unsigned long long *bar) {
+  const int N = B.nzm, nh = B.nymh, L = fft_z_lines(B), rb = B.fz_rb;
   const int ntl = (nh + L - 1) / L;
   const int k = lt / ntl, ky0 = (lt - k * ntl) * L;
-  const double2 *spec = B.spec + (long long)k * N * nh;
-  for (int t = threadIdx.x; t < L * N; t += FFT_T) {
-    const int l = t % L, n = t / L;
-    if (ky0 + l < nh) cp_async16(a + t, spec + (long long)n * nh + ky0 + l);
-    else a[t] = make_double2(0.0, 0.0);
-  }
+  mbar_expect_tx(bar, (unsigned)(16 * L * N));
+  for (int c = 0; c < N / rb; ++c) tma_load_2d(a + c * rb * L, B.tm_z, bar, 2 * ky0, k * N + c * rb);
 }
 
 template <int SGN>
@@ -432,21 +436,25 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
   extern __shared__ double2 fsm[];
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
-  int t = blockIdx.x, loaded = -1, lt;
-  if (t < total) {
-    const int b = tile_box(bt, t, lt);
-    fft_z_copy_in(bt.boxes[b], lt, slot[0]);
+  unsigned long long *bar = (unsigned long long *)(tws + sm.tw);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
   }
-  cp_async_commit();
+  __syncthreads();
+  int t = blockIdx.x, loaded = -1, lt;
+  if (t < total && threadIdx.x == 0) {
+    const int b = tile_box(bt, t, lt);
+    fft_z_issue(bt.boxes[b], lt, slot[0], &bar[0]);
+  }
   for (int it = 0; t < total; ++it, t += gridDim.x) {
     const int tn = t + gridDim.x;
-    if (tn < total) {
+    if (tn < total && threadIdx.x == 0) {
       int ln;
       const int bn = tile_box(bt, tn, ln);
-      fft_z_copy_in(bt.boxes[bn], ln, slot[(it + 1) & 1]);
+      fft_z_issue(bt.boxes[bn], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
     }
-    cp_async_commit();
-    cp_async_wait_1();
     const int b = tile_box(bt, t, lt);
     const BoxDev &B = bt.boxes[b];
     const bool run = B.active && ns < B.nsst && B.sc->status == 0;
@@ -454,7 +462,16 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
       for (int q = threadIdx.x; q < B.nzm; q += FFT_T) tws[q] = __ldg(B.twz + q);
       loaded = b;
     }
-    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      // a copy did not complete: flag the box, let the other slot's copy
+      // (if any) finish within the same bound, and stop this block
+      if (threadIdx.x == 0) {
+        atomicExch(&B.sc->status, AFID_STATUS_DEVICE_TIMEOUT);
+        if (tn < total) mbar_wait_bounded(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+      }
+      return;
+    }
     if (run) {
       const int N = B.nzm, nh = B.nymh, L = fft_z_lines(B);
       const int ntl = (nh + L - 1) / L;
@@ -462,8 +479,10 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
       double2 *cur = slot[it & 1];
       const int lgL = ilog2(L);
       fft_tile<true, SGN>(cur, N, lgL, B.fft_z_radix, B.fft_z_np, tws, SmemSrc{cur, lgL},
-                            ZDst{B.spec + (long long)k * N * nh, nh, ky0});
+                          ZDst{B.spec + (long long)k * N * nh, nh, ky0});
     }
+    // the slot is refilled by TMA in the next iteration
+    fence_proxy_async_smem();
     __syncthreads();
   }
 }
