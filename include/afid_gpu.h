@@ -22,6 +22,9 @@
  *     reference's error code in afid_box_scalars.status (165 CFL too large,
  *     166 dt < dtmin, 169 divergence > resid, 266 velocity limit or a
  *     non-finite value; main.F90:184-220) and is skipped by later launches.
+ *     Status 990 (no counterpart in the reference) marks a box whose
+ *     asynchronous tile copy did not complete within the kernel's wait
+ *     limit; the kernel stops instead of waiting further.
  *   - One host thread per context; calls on a context are not re-entrant.
  *   - All work is queued on the context's stream; functions that return
  *     host data synchronise that stream.
