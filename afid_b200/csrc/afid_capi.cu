@@ -47,7 +47,7 @@ int fail(int code, const char *fmt, ...) {
       return fail(AFID_ECUDA, "launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
-enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, NFAM };
+enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, FAM_K2, NFAM };
 constexpr int HIST_CAP = 4096;
 
 struct HostBox {
@@ -72,6 +72,7 @@ struct Batch {
   size_t smem_y = 0, smem_z = 0;
   FftSmem sm_y{0, 0}, sm_z{0, 0};   // slot and twiddle sizes of the persistent transforms
   int grid_y = 0, grid_z = 0;       // their resident grids
+  int k2_block = 256;               // threads per block of the back-substitution kernel
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
   int k1_minb = 2;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
@@ -108,8 +109,9 @@ int factor_radices(int n, int *rad, int *np) {
 constexpr int K1_VMIN = 2, K1_VMAX = 8;
 int k1_tile_height(int variant) { return (variant == 5 || variant >= 7) ? 4 : variant == 6 ? 2 : 8; }
 
-long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2) {
+long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 256) {
   switch (fam) {
+    case FAM_K2: return cdiv(B.plane, k2_block);
     case FAM_K1: return cdiv(B.nym, K1_TJ) * cdiv(B.nzm, k1_tile_height(k1_variant));
     case FAM_COL: return cdiv(B.plane, 256);
     case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
@@ -358,6 +360,36 @@ int fft_grid(K kernel, size_t smem, int tiles, int *grid) {
   return 0;
 }
 
+// Block size of the back-substitution kernel.  Each of its threads marches
+// a whole column, so the grid runs in waves of (SMs x resident threads)
+// columns and a last, partly filled wave costs a full column march.  Of the
+// block sizes that keep the SMs' thread slots filled, pick the one whose
+// waves are filled best (ties: more resident threads).
+int k2_block_size(const std::vector<BoxDev> &devs, int *out) {
+  int dev = 0, nsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  double best = 1e30;
+  int best_res = 0;
+  *out = 256;
+  for (int bs = 128; bs <= 256; bs += 32) {
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_implicit_bwd, bs, 0));
+    if (occ < 1) continue;
+    const long long res = (long long)nsm * occ * bs;   // resident threads
+    long long cols = 0;
+    for (const BoxDev &d : devs) cols += cdiv(d.plane, bs) * bs;
+    const double waves = (double)cols / (double)res;
+    const double cost = std::ceil(waves) / waves;   // >= 1: time over the ideal
+    if (cost < best - 1e-9 || (cost < best + 1e-9 && res > best_res)) {
+      best = cost;
+      best_res = (int)(res / nsm);
+      *out = bs;
+    }
+  }
+  return 0;
+}
+
 int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   if (n <= 0 || !ids) return fail(AFID_EINVAL, "empty box set");
   std::vector<int> key(ids, ids + n);
@@ -390,11 +422,15 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     const char *e = getenv("AFID_K1_VARIANT");
     if (e && atoi(e) >= K1_VMIN && atoi(e) <= K1_VMAX) bt->k1_minb = atoi(e);
   }
+  {
+    int rc = k2_block_size(devs, &bt->k2_block);
+    if (rc) { delete bt; return rc; }
+  }
   for (int f = 0; f < NFAM; ++f) {
     long long acc = 0;
     for (int b = 0; b < n; ++b) {
       off[(size_t)f * (n + 1) + b] = (int)acc;
-      acc += tiles_of(devs[b], f, bt->k1_minb);
+      acc += tiles_of(devs[b], f, bt->k1_minb, bt->k2_block);
     }
     if (acc > 0x7fffffffLL) { delete bt; return fail(AFID_ESIZE, "grid too large"); }
     off[(size_t)f * (n + 1) + n] = (int)acc;
@@ -512,7 +548,7 @@ int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) 
   }
   CKL();
   PMARK(pf, AFID_K_EXPLICIT_FWD);
-  k_implicit_bwd<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
+  k_implicit_bwd<<<bt->total[FAM_K2], bt->k2_block, 0, s>>>(bdev(bt, FAM_K2), ns);
   CKL();
   PMARK(pf, AFID_K_IMPLICIT_BWD);
   int rc = launch_poisson(bt, s, ns, true, pf);
