@@ -133,7 +133,7 @@ Sizes sizes_of(const afid_box_params &p) {
   s.plane = (long long)p.nym * p.nzm;
   s.fsize = s.nx * s.plane;
   s.nspec = (long long)p.nxm * p.nzm * (p.nym / 2 + 1);
-  long long pois = 3 * s.nspec + (long long)p.nxm * s.plane;
+  long long pois = 3 * s.nspec + 1 + (long long)p.nxm * s.plane;   // dph 16-byte aligned
   s.scratch = pois > 4 * s.fsize ? pois : 4 * s.fsize;
   // tables + twiddles + coef + nu partials + history + scalars (in doubles)
   s.small = (long long)T_NK * s.nx + p.nzm + p.nym + 2LL * (p.nym + p.nzm) +
@@ -409,7 +409,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     devs.push_back(d);
     fft_smem_grow(d, bt->sm_y, bt->sm_z, twy_max, twz_max);
   }
-  bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16;
+  bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16 + 16;   // + two mbarriers
   bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16 + 16;   // + two mbarriers
   {
     // one variant of the explicit/forward kernel per launch: the one the
@@ -784,7 +784,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   for (int q = 0; q < 4; ++q) d.ybuf[q] = Sc + q * s.fsize;
   d.spec = (double2 *)Sc;
   d.dstore = Sc + 2 * s.nspec;
-  d.phi = Sc + 3 * s.nspec;
+  d.phi = Sc + ((3 * s.nspec + 1) & ~1LL);   // 16-byte aligned rows for the bulk copies
   hb->scratch_doubles = (size_t)s.scratch;
   // small allocations
   double *M = (double *)hb->mem_small;
@@ -1515,6 +1515,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
                 "noalloc: box %dx%dx%d exceeds the fixed scratch: nxm <= %d, nym, nzm <= %d and "
                 "nxm*nzm*(nym/2+1) <= %lld (got %lld)",
                 nxm, nym, nzm, NOALLOC_MAX_NXM, NOALLOC_MAX_NYZ, NOALLOC_MAX_SPEC, nspec);
+  if ((uintptr_t)dph & 15) return fail(AFID_EINVAL, "noalloc: dph must be 16-byte aligned");
   for (int k = 1; k <= nxm; ++k)
     if (!(xc[k] > xc[k - 1])) return fail(AFID_EINVAL, "noalloc: xc must be increasing");
   BoxDev d;
@@ -1616,7 +1617,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   FftSmem smy{0, 0}, smz{0, 0};
   int twy = 0, twz = 0, gy = 0, gz = 0;
   fft_smem_grow(d, smy, smz, twy, twz);
-  const size_t sy = (size_t)(2 * smy.slot + twy) * 16;
+  const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + 16;
   const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + 16;
   rc = fft_grid(k_fft_y_fwd, sy, off[0][1], &gy);
   if (!rc) rc = fft_grid(k_fft_z<-1>, sz, off[1][1], &gz);

@@ -198,6 +198,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsig
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+// 1-D bulk copy of ``bytes`` (a multiple of 16) from global src to shared
+// dst, both 16-byte aligned, completed on ``bar``
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
 // 2-D tile load of box (x, y) of ``map`` into shared memory at dst (16-byte
 // aligned); x times the element size must be a multiple of 16 bytes
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x,

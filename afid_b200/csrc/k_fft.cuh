@@ -276,8 +276,8 @@ constexpr int FFT_MAX_LINES = 16;
 
 // y: a slot holds the 2 Pp real rows of a forward tile (Pp N complex) or the
 // 2 Pp half-spectrum rows of an inverse tile (2 Pp (N/2+1) complex)
-__host__ __device__ __forceinline__ int fft_y_slot(int N, int Pp) { return 2 * Pp * (N / 2 + 1); }  // >= Pp (N + 1)
-__host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 * fft_y_slot(N, Pp) + N) * 16; }
+__host__ __device__ __forceinline__ int fft_y_slot(int N, int Pp) { return 2 * Pp * (N / 2 + 1); }  // = Pp (N + 2)
+__host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 * fft_y_slot(N, Pp) + N) * 16 + 16; }
 __host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16 + 16; }
 __host__ __device__ __forceinline__ bool fft_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
 __host__ __device__ __forceinline__ bool fft_y_ok(int N, int Pp, int budget) {
@@ -327,8 +327,9 @@ __device__ __forceinline__ int tile_box(const BatchDev &bt, int tile, int &local
 struct NoDst {
   __device__ __forceinline__ void operator()(int, int, double2) const {}
 };
-// rows are copied in with a stride of nym + 1 doubles, which spreads the
-// rows of one column over the shared-memory banks
+// rows are copied in with a stride of nym + 2 doubles, which spreads the
+// rows of one column over the shared-memory banks and keeps every row
+// 16-byte aligned
 struct PairSrc {
   const double *rows; int RS;
   __device__ __forceinline__ double2 operator()(int p, int n) const {
@@ -336,37 +337,50 @@ struct PairSrc {
   }
 };
 
-__device__ __forceinline__ void fft_y_fwd_copy_in(const BoxDev &B, int lt, double *rows) {
+// Copy-in of a y tile: one bulk copy per row (issued by one thread,
+// completed on the slot's mbarrier); rows beyond nzm are zeroed by the block.
+__device__ __forceinline__ void fft_y_fwd_issue(const BoxDev &B, int lt, double *rows, unsigned long long *bar) {
   const int N = B.nym, nzm = B.nzm, Pp = fft_y_pairs(B);
   const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
   const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
+  const int nr = min(2 * Pp, nzm - i0);
+  mbar_expect_tx(bar, (unsigned)(nr * N * 8));
   const double *phik = B.phi + (long long)k * B.plane;
-  for (int t = threadIdx.x; t < 2 * Pp * N; t += FFT_T) {
-    const int r = t / N, j = t - r * N;
-    if (i0 + r < nzm) cp_async8d(rows + r * (N + 1) + j, phik + (long long)(i0 + r) * N + j);
-    else rows[r * (N + 1) + j] = 0.0;
-  }
+  for (int r = 0; r < nr; ++r) bulk_load(rows + r * (N + 2), phik + (long long)(i0 + r) * N, (unsigned)(N * 8), bar);
+}
+__device__ __forceinline__ void fft_y_fwd_zero_tail(const BoxDev &B, int lt, double *rows) {
+  const int N = B.nym, nzm = B.nzm, Pp = fft_y_pairs(B);
+  const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
+  const int i0 = (lt - (lt / groups) * groups) * 2 * Pp;
+  for (int r = max(nzm - i0, 0); r < 2 * Pp; ++r)
+    for (int j = threadIdx.x; j < N; j += FFT_T) rows[r * (N + 2) + j] = 0.0;
 }
 
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, FftSmem sm, int total) {
   extern __shared__ double2 fsm[];
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
+  unsigned long long *bar = (unsigned long long *)(tws + sm.tw);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
   int t = blockIdx.x, loaded = -1, lt;
   if (t < total) {
     const int b = tile_box(bt, t, lt);
-    fft_y_fwd_copy_in(bt.boxes[b], lt, (double *)slot[0]);
+    if (threadIdx.x == 0) fft_y_fwd_issue(bt.boxes[b], lt, (double *)slot[0], &bar[0]);
+    fft_y_fwd_zero_tail(bt.boxes[b], lt, (double *)slot[0]);
   }
-  cp_async_commit();
   for (int it = 0; t < total; ++it, t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tn < total) {
       int ln;
       const int bn = tile_box(bt, tn, ln);
-      fft_y_fwd_copy_in(bt.boxes[bn], ln, (double *)slot[(it + 1) & 1]);
+      if (threadIdx.x == 0) fft_y_fwd_issue(bt.boxes[bn], ln, (double *)slot[(it + 1) & 1], &bar[(it + 1) & 1]);
+      fft_y_fwd_zero_tail(bt.boxes[bn], ln, (double *)slot[(it + 1) & 1]);
     }
-    cp_async_commit();
-    cp_async_wait_1();
     const int b = tile_box(bt, t, lt);
     const BoxDev &B = bt.boxes[b];
     const bool run = B.active && ns < B.nsst && B.sc->status == 0;
@@ -374,15 +388,22 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
       for (int q = threadIdx.x; q < B.nym; q += FFT_T) tws[q] = __ldg(B.twy + q);
       loaded = b;
     }
-    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(&B.sc->status, AFID_STATUS_DEVICE_TIMEOUT);
+        if (tn < total) mbar_wait_bounded(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+      }
+      return;
+    }
     if (run) {
       const int N = B.nym, nzm = B.nzm, Pp = fft_y_pairs(B), nh = B.nymh;
       const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
       const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
       double2 *cur = slot[it & 1];
       const int lgP = ilog2(Pp);
-      fft_tile<false, -1>(cur, N, lgP, B.fft_y_radix, B.fft_y_np, tws, PairSrc{(const double *)cur, N + 1},
-                      NoDst{});
+      fft_tile<false, -1>(cur, N, lgP, B.fft_y_radix, B.fft_y_np, tws, PairSrc{(const double *)cur, N + 2},
+                          NoDst{});
       // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
       // B = (Z_q - conj Z_{N-q}) / (2i)
       for (int u = threadIdx.x; u < Pp * nh; u += FFT_T) {
@@ -398,6 +419,8 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
         if (i + 1 < nzm) B.spec[base + nh] = Bv;
       }
     }
+    // the slot is refilled by bulk copies in the next iteration
+    fence_proxy_async_smem();
     __syncthreads();
   }
 }
@@ -608,37 +631,51 @@ struct YInvDst {
 // coefficients are ignored.  A tile's 2 Pp half-spectrum rows are copied
 // into a slot; two rows are recovered from one complex line Z = A + i B,
 // which the first pass writes over the raw rows it has read.
-__device__ __forceinline__ void fft_y_inv_copy_in(const BoxDev &B, int lt, double2 *raw) {
+// Copy-in of an inverse y tile: one bulk copy per half-spectrum row (issued
+// by one thread, completed on the slot's mbarrier); rows beyond nzm are
+// zeroed by the block.
+__device__ __forceinline__ void fft_y_inv_issue(const BoxDev &B, int lt, double2 *raw, unsigned long long *bar) {
   const int nzm = B.nzm, nh = B.nymh, Pp = fft_y_pairs(B);
   const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
   const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
+  const int nr = min(2 * Pp, nzm - i0);
+  mbar_expect_tx(bar, (unsigned)(nr * nh * 16));
   const double2 *speck = B.spec + (long long)k * nzm * nh;
-  for (int t = threadIdx.x; t < 2 * Pp * nh; t += FFT_T) {
-    const int r = t / nh, q = t - r * nh;
-    if (i0 + r < nzm) cp_async16(raw + t, speck + (long long)(i0 + r) * nh + q);
-    else raw[t] = make_double2(0.0, 0.0);
-  }
+  for (int r = 0; r < nr; ++r) bulk_load(raw + r * nh, speck + (long long)(i0 + r) * nh, (unsigned)(nh * 16), bar);
+}
+__device__ __forceinline__ void fft_y_inv_zero_tail(const BoxDev &B, int lt, double2 *raw) {
+  const int nzm = B.nzm, nh = B.nymh, Pp = fft_y_pairs(B);
+  const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
+  const int i0 = (lt - (lt / groups) * groups) * 2 * Pp;
+  for (int r = max(nzm - i0, 0); r < 2 * Pp; ++r)
+    for (int q = threadIdx.x; q < nh; q += FFT_T) raw[r * nh + q] = make_double2(0.0, 0.0);
 }
 
 __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, FftSmem sm, int total) {
   extern __shared__ double2 fsm[];
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
+  unsigned long long *bar = (unsigned long long *)(tws + sm.tw);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
   int t = blockIdx.x, loaded = -1, lt;
   if (t < total) {
     const int b = tile_box(bt, t, lt);
-    fft_y_inv_copy_in(bt.boxes[b], lt, slot[0]);
+    if (threadIdx.x == 0) fft_y_inv_issue(bt.boxes[b], lt, slot[0], &bar[0]);
+    fft_y_inv_zero_tail(bt.boxes[b], lt, slot[0]);
   }
-  cp_async_commit();
   for (int it = 0; t < total; ++it, t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tn < total) {
       int ln;
       const int bn = tile_box(bt, tn, ln);
-      fft_y_inv_copy_in(bt.boxes[bn], ln, slot[(it + 1) & 1]);
+      if (threadIdx.x == 0) fft_y_inv_issue(bt.boxes[bn], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
+      fft_y_inv_zero_tail(bt.boxes[bn], ln, slot[(it + 1) & 1]);
     }
-    cp_async_commit();
-    cp_async_wait_1();
     const int b = tile_box(bt, t, lt);
     const BoxDev &B = bt.boxes[b];
     const bool run = B.active && ns < B.nsst && B.sc->status == 0;
@@ -646,15 +683,23 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, Fft
       for (int q = threadIdx.x; q < B.nym; q += FFT_T) tws[q] = __ldg(B.twy + q);
       loaded = b;
     }
-    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(&B.sc->status, AFID_STATUS_DEVICE_TIMEOUT);
+        if (tn < total) mbar_wait_bounded(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+      }
+      return;
+    }
     if (run) {
       const int N = B.nym, nzm = B.nzm, nh = B.nymh, Pp = fft_y_pairs(B);
       const int groups = (nzm + 2 * Pp - 1) / (2 * Pp);
       const int k = lt / groups, i0 = (lt - k * groups) * 2 * Pp;
       double2 *cur = slot[it & 1];
       fft_tile<true, +1>(cur, N, ilog2(Pp), B.fft_y_radix, B.fft_y_np, tws, YInvSmemSrc{cur, N, nh, (N % 2) == 0},
-                           YInvDst{B.phi + (long long)k * B.plane, N, nzm, i0});
+                         YInvDst{B.phi + (long long)k * B.plane, N, nzm, i0});
     }
+    fence_proxy_async_smem();
     __syncthreads();
   }
 }

@@ -237,7 +237,8 @@ int afid_slab_dump(afid_ctx *ctx, int box_id, const int *kslab, int nslab, doubl
  * on every GPU that loads the library until exit).  No cudaMalloc, cudaFree or
  * other allocating call is made.
  *   dph    device pointer, in/out: nxm*nym*nzm doubles in the library's
- *          device layout dph[k][i][j] (y fastest, then z, then x)
+ *          device layout dph[k][i][j] (y fastest, then z, then x), 16-byte
+ *          aligned (as every cudaMalloc result is)
  *   xc     host pointer: the nx = nxm+1 node positions
  *   stream cudaStream_t to queue the work on (0: the default stream)
  * Limits: nxm <= 1024, nym and nzm <= 3072 (nym even, prime factors <= 7),

@@ -62,3 +62,13 @@ def test_noalloc_rejects_oversize():
         C.c_void_p(1), 512, 1024, 1024, _lib.dptr(xc), 1.0, 1.0, 1.0, None)
     assert rc == -6
     assert b"exceeds the fixed scratch" in _lib.lib().afid_last_error()
+
+
+def test_noalloc_rejects_misaligned_dph():
+    """The bulk copies of the transforms need a 16-byte aligned dph; a
+    misaligned pointer is refused on the host before any device work."""
+    xc = np.linspace(0.0, 1.0, 33)
+    rc = _lib.lib().afid_solve_pressure_correction_noalloc(
+        C.c_void_p(8), 32, 16, 16, _lib.dptr(xc), 1.0, 1.0, 1.0, None)
+    assert rc == -1
+    assert b"16-byte aligned" in _lib.lib().afid_last_error()
