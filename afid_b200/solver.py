@@ -94,8 +94,13 @@ class Context:
         _lib.check(self._L.afid_ctx_synchronize(self.h))
 
     # -- boxes
-    def add_box(self, cfg: BouIn, xc: np.ndarray | None = None) -> "Box":
-        cfg.validate()
+    def add_box(self, cfg: BouIn, xc: np.ndarray | None = None, validate: bool = True) -> "Box":
+        """A box for ``cfg``.  ``validate`` applies the reference's start-up
+        checks (ReadInputFile/main.F90); without it only the library's own
+        limits apply (e.g. its transforms also take a largest factor of 7,
+        which the reference's Factorize rejects)."""
+        if validate:
+            cfg.validate()
         if xc is None:
             xc = make_grid(cfg.nxm, cfg.istr3, cfg.str3, cfg.alx3)
         xc = np.ascontiguousarray(xc, dtype=np.float64)

@@ -28,6 +28,12 @@ def _box(ctx, cfg, s):
     ((32, 48, 32), dict(ray=1e7, pra=1.0, ylen=1.5)),
     ((20, 20, 40), dict(ray=3e6, pra=4.38, ylen=1.0, zlen=2.0)),
     ((16, 32, 16), dict(ray=1e6, inslws=0, inslwn=0, istr3=6, str3=2.0)),
+    # odd nzm (a y tile with a tail row), nym below one 32-wide tile, radix 5
+    ((18, 30, 45), dict(ray=2e6, pra=1.0, ylen=1.2, zlen=1.8)),
+    # radix 5 along y and z, a partial 32-wide tile along y
+    ((12, 50, 20), dict(ray=5e5, pra=0.7, ylen=2.0, zlen=0.8)),
+    # radix 16 x 5 along z, three 32-wide tiles along y
+    ((24, 96, 80), dict(ray=1e7, pra=1.0, ylen=1.2, zlen=1.0)),
 ])
 def test_fused_step_matches_oracle(ctx, shape, kw):
     cfg = cfg_of(*shape, dt=5e-4, **kw)
@@ -163,3 +169,20 @@ def test_full_size_box_properties(ctx):
     assert box.check_divergence() <= 1e-10
     assert box.scalars()["status"] == 0
     ctx.remove_box(box)
+
+
+def test_radix7_transforms_match_oracle(ctx):
+    """The library's transforms also take a largest factor of 7 (the
+    reference's Factorize rejects those sizes, so bou.in validation is
+    bypassed here): nym = 70 (a partial 32-wide tile), nzm = 14."""
+    cfg = cfg_of(12, 70, 14, dt=5e-4, ray=5e5, pra=0.7, ylen=2.0, zlen=0.4)
+    s = oracle_state(cfg, seed=1)
+    box = ctx.add_box(cfg, s.g.xc, validate=False)
+    for f in FIELDS:
+        box.upload(f, getattr(s, f))
+    O.run(s, 1, cfg.dt)
+    ctx.step([box], 1)
+    err = compare_fields(box, s)
+    assert all(v <= 1e-11 for v in err.values()), err
+    ctx.remove_box(box)
+
