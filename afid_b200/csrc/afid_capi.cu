@@ -462,9 +462,14 @@ BatchDev bdev(const Batch *bt, int fam) {
   return d;
 }
 
+// The shared-memory attributes apply per device: set them once on each
+// device the process uses (the current one).
 int init_kernel_attrs() {
-  static bool done = false;
-  if (done) return 0;
+  static bool done[64] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(AFID_EINVAL, "device %d out of range", dev);
+  if (done[dev]) return 0;
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 8>::SMEM));
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<1, 8>::SMEM));
   CK(cudaFuncSetAttribute(k_explicit_implicit_fwd<8, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, K1Ring<2, 8>::SMEM));
@@ -477,7 +482,7 @@ int init_kernel_attrs() {
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  done = true;
+  done[dev] = true;
   return 0;
 }
 

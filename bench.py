@@ -231,7 +231,7 @@ def reference_arm(args):
     conf = dict(conf)
     conf["cpu_sample"] = desc
     line = {
-        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0, "steps": steps,
+        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": tps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": conf, "impl": "reference",
