@@ -738,7 +738,7 @@ int afid_make_grid(int nxm, int istr3, double str3, double alx3, double *xc) {
 size_t afid_box_device_bytes(const afid_box_params *p) {
   if (!p) return 0;
   Sizes s = sizes_of(*p);
-  return (size_t)(9 * s.fsize + s.scratch + s.small) * sizeof(double) + 2 * sizeof(BoxDev) + 4096;
+  return (size_t)(9 * s.fsize + s.scratch + s.nspec + s.small) * sizeof(double) + 2 * sizeof(BoxDev) + 4096;
 }
 
 int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *box_id) {
@@ -773,7 +773,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   d.hist_cap = HIST_CAP;
   d.k1_minb = 2;
   const size_t fb = 9 * (size_t)s.fsize * sizeof(double);
-  const size_t sb = (size_t)s.scratch * sizeof(double);
+  const size_t sb = (size_t)(s.scratch + s.nspec) * sizeof(double);   // + the Poisson pivot table
   const size_t mb = (size_t)s.small * sizeof(double);
   if (cudaMalloc(&hb->mem_fields, fb) != cudaSuccess || cudaMalloc(&hb->mem_scratch, sb) != cudaSuccess ||
       cudaMalloc(&hb->mem_small, mb) != cudaSuccess || cudaMalloc(&hb->d_self, sizeof(BoxDev)) != cudaSuccess) {
@@ -788,7 +788,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   double *Sc = (double *)hb->mem_scratch;
   for (int q = 0; q < 4; ++q) d.ybuf[q] = Sc + q * s.fsize;
   d.spec = (double2 *)Sc;
-  d.dstore = Sc + 2 * s.nspec;
+  d.dstore = Sc + s.scratch;                 // pivot table, outside the aliased scratch
   d.phi = Sc + ((3 * s.nspec + 1) & ~1LL);   // 16-byte aligned rows for the bulk copies
   hb->scratch_doubles = (size_t)s.scratch;
   // small allocations
@@ -826,8 +826,13 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
             cudaMemsetAsync(hb->mem_small, 0, mb, st) == cudaSuccess &&
             cudaMemcpyAsync((void *)d.tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync((void *)d.twy, tw.data(), tw.size() * 16, cudaMemcpyHostToDevice, st) == cudaSuccess &&
-            cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st) == cudaSuccess &&
-            cudaStreamSynchronize(st) == cudaSuccess;
+            cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  if (ok) {   // the Poisson pivots depend on the grid only: tabulate them once
+    const long long nmode = (long long)p->nzm * d.nymh;
+    k_poisson_pivots<<<(unsigned)((nmode + 255) / 256), 256, 0, st>>>(d);
+    ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
+    d.piv_ready = 1;
+  }
   if (!ok) {
     cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small); cudaFree(hb->d_self);
     delete hb;

@@ -76,6 +76,7 @@ struct BoxDev {
   // and the correction)
   double2 *spec;        // [k][kz][ky], k < nxm, ky <= nym/2
   double *dstore;       // Thomas pivots of the Poisson solve, same indexing
+                        // (a table of its own when piv_ready, else scratch)
   double *phi;          // pressure correction dph, [k][i][j], k < nxm
   // reference-boundary mode buffers (allocated on first use)
   double *qcap, *dq, *hro, *rhs;
@@ -98,7 +99,7 @@ struct BoxDev {
   int fz_lines;         // tuning: ky columns per z-FFT block (0 = default)
   int fz_rb;            // kz rows per TMA box of the z transform (a divisor of nzm, <= 256)
   const CUtensorMap *tm_z;  // TMA map of spec as a 2-D FP64 array (2*nymh x nxm*nzm), box 2L x fz_rb
-  int pad2_;
+  int piv_ready;        // 1 = dstore holds the Poisson pivots of this grid (tabulated once)
 };
 
 // Work decomposition: each kernel family launches a 1-D grid over the

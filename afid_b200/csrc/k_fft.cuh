@@ -523,7 +523,46 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
 // ---------------------------------------------------------------------------
 constexpr int KP_U = 4;   // planes per prefetch chunk of the sweeps
 
-__global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
+// Row scale s(k) of mode (ak, ak1) and one step of the pivot recurrence
+// (zgttrf without pivoting): for row k >= 1 with am = amph(k) s(k),
+//   fact = am / d(k-1),  d(k) = 1 - fact * ap(k-1),  ap(k-1) = apph(k-1) s(k-1).
+// The sweep and the kernel that tabulates the pivots both go through these,
+// so the table holds the bits the sweep would compute.
+__device__ __forceinline__ double px_scale(const double *acph, int k, double ak, double ak1) {
+  return 1.0 / ((__ldg(acph + k) - ak) - ak1);
+}
+__device__ __forceinline__ double px_pivot(double am, double ap_prev, double &d) {
+  const double fact = am / d;
+  d = 1.0 - fact * ap_prev;
+  return fact;
+}
+
+// Pivots d(k) of every mode of one box, written to B.dstore in the sweep's
+// indexing.  They depend on the grid only, so a box computes them once.
+__global__ void __launch_bounds__(256) k_poisson_pivots(BoxDev B) {
+  const int nh = B.nymh, nzm = B.nzm, nxm = B.nxm;
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nmode = (long long)nzm * nh;
+  if (m >= nmode) return;
+  const int kz = (int)(m / nh), ky = (int)(m - (long long)kz * nh);
+  const double ak = __ldg(B.tab + (long long)T_NK * B.nx + nzm + ky);
+  const double ak1 = __ldg(B.tab + (long long)T_NK * B.nx + kz);
+  const double *amph = B.tab + (long long)T_AMPHK * B.nx;
+  const double *acph = B.tab + (long long)T_ACPHK * B.nx;
+  const double *apph = B.tab + (long long)T_APPHK * B.nx;
+  double *__restrict__ dst = B.dstore + m;
+  double d = 1.0, ap_prev = 0.0;
+  for (int k = 0; k < nxm; ++k) {
+    const double s = px_scale(acph, k, ak, ak1);
+    if (k > 0) px_pivot(__ldg(amph + k) * s, ap_prev, d);
+    dst[(long long)k * nmode] = d;
+    ap_prev = __ldg(apph + k) * s;
+  }
+}
+
+// Four resident blocks per SM (64 registers): the sweep is a chain of
+// dependent divisions per mode, so more modes in flight hide more of it.
+__global__ void __launch_bounds__(256, 4) k_poisson_x(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
@@ -542,6 +581,7 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
   double *__restrict__ dst = B.dstore + m;
   const long long st = nmode;
   const bool zero_mode = (ky == 0 && kz == 0);
+  const bool store_d = !B.piv_ready;             // else the pivots are tabulated already
   const double norm = (double)(B.nzm * B.nym);   // the forward transforms' 1/(nym nzm)
   // forward elimination (dgttrf + dgttrs forward sweep), planes in chunks
   double d = 1.0, ap_prev = 0.0;
@@ -555,21 +595,19 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
     for (int u = 0; u < KP_U; ++u) {
       const int k = k0 + u;
       if (k >= nxm) break;
-      const double s = 1.0 / ((__ldg(acph + k) - ak) - ak1);
+      const double s = px_scale(acph, k, ak, ak1);
       double2 rk = r[u];
       rk.x = rk.x / norm; rk.y = rk.y / norm;
       rk.x = rk.x * s; rk.y = rk.y * s;
       if (k == 0) {
         y = rk;
       } else {
-        const double am = __ldg(amph + k) * s;
-        const double fact = am / d;
-        d = 1.0 - fact * ap_prev;
+        const double fact = px_pivot(__ldg(amph + k) * s, ap_prev, d);
         y.x = rk.x - fact * y.x;
         y.y = rk.y - fact * y.y;
       }
       x[(long long)k * st] = y;
-      dst[(long long)k * st] = d;
+      if (store_d) dst[(long long)k * st] = d;
       ap_prev = __ldg(apph + k) * s;
     }
   }
@@ -594,7 +632,7 @@ __global__ void __launch_bounds__(256) k_poisson_x(BatchDev bt, int ns) {
     for (int u = 0; u < KP_U; ++u) {
       const int k = k0 - u;
       if (k < 0) break;
-      const double sk = 1.0 / ((__ldg(acph + k) - ak) - ak1);
+      const double sk = px_scale(acph, k, ak, ak1);
       const double ap = __ldg(apph + k) * sk;
       xn.x = (yk[u].x - ap * xn.x) / dk[u];
       xn.y = (yk[u].y - ap * xn.y) / dk[u];
