@@ -49,12 +49,15 @@ SMEM_MAX = 200 * 1024   # shared memory of one transform block (two copy-in slot
 TILE_MAX = 14 * 256     # complex values of one in-place tile
 
 
+TAIL_BYTES = 1024        # upper bound of the slot mbarriers and the cached box descriptor
+
+
 def fft_y_bytes(n: int, pairs: int) -> int:
-    return (2 * 2 * pairs * (n // 2 + 1) + n) * 16
+    return (2 * 2 * pairs * (n // 2 + 1) + n) * 16 + TAIL_BYTES
 
 
 def fft_z_bytes(n: int, lines: int) -> int:
-    return (2 * lines * n + n) * 16
+    return (2 * lines * n + n) * 16 + TAIL_BYTES
 
 
 def candidates(cfg: BouIn) -> dict:

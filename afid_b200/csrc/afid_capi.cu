@@ -409,8 +409,8 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     devs.push_back(d);
     fft_smem_grow(d, bt->sm_y, bt->sm_z, twy_max, twz_max);
   }
-  bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16 + 16;   // + two mbarriers
-  bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16 + 16;   // + two mbarriers
+  bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16 + FFT_TAIL_BYTES;   // + mbarriers, descriptor
+  bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16 + FFT_TAIL_BYTES;
   {
     // one variant of the explicit/forward kernel per launch: the one the
     // boxes holding most of the cells ask for
@@ -1627,8 +1627,8 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   FftSmem smy{0, 0}, smz{0, 0};
   int twy = 0, twz = 0, gy = 0, gz = 0;
   fft_smem_grow(d, smy, smz, twy, twz);
-  const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + 16;
-  const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + 16;
+  const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + FFT_TAIL_BYTES;
+  const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + FFT_TAIL_BYTES;
   rc = fft_grid(k_fft_y_fwd, sy, off[0][1], &gy);
   if (!rc) rc = fft_grid(k_fft_z<-1>, sz, off[1][1], &gz);
   if (rc) return rc;

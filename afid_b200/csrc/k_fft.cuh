@@ -277,8 +277,15 @@ constexpr int FFT_MAX_LINES = 16;
 // y: a slot holds the 2 Pp real rows of a forward tile (Pp N complex) or the
 // 2 Pp half-spectrum rows of an inverse tile (2 Pp (N/2+1) complex)
 __host__ __device__ __forceinline__ int fft_y_slot(int N, int Pp) { return 2 * Pp * (N / 2 + 1); }  // = Pp (N + 2)
-__host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 * fft_y_slot(N, Pp) + N) * 16 + 16; }
-__host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16 + 16; }
+// Dynamic shared memory of a transform block: two slots, the twiddles, then
+// the two slot mbarriers (16 bytes) and the cached box descriptor.  The
+// slots come first, at the start of the dynamic region, which keeps the TMA
+// destinations aligned (the block has no static shared memory).
+constexpr int FFT_DESC_BYTES = (int)((sizeof(BoxDev) + 15) / 16 * 16);
+constexpr int FFT_TAIL_BYTES = 16 + FFT_DESC_BYTES;
+static_assert(FFT_TAIL_BYTES <= 1024, "the autotuner's size bound assumes a tail of at most 1 KB");
+__host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 * fft_y_slot(N, Pp) + N) * 16 + FFT_TAIL_BYTES; }
+__host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16 + FFT_TAIL_BYTES; }
 __host__ __device__ __forceinline__ bool fft_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
 __host__ __device__ __forceinline__ bool fft_y_ok(int N, int Pp, int budget) {
   return fft_pow2(Pp) && Pp * N <= FFT_TILE_MAX && fft_y_bytes(N, Pp) <= budget;
@@ -316,6 +323,19 @@ __device__ __forceinline__ int tile_box(const BatchDev &bt, int tile, int &local
   const int b = find_box(bt.tile_off, bt.nbox, tile);
   local = tile - __ldg(bt.tile_off + b);
   return b;
+}
+
+// A transform block keeps the descriptor of the box it is working on in
+// shared memory, next to that box's twiddles, and reloads both when a tile
+// of another box comes up.  Read from global memory, every descriptor field
+// after a global store would be reloaded (the store might alias it), and
+// each reload is a dependent trip to the L2.  The block's threads copy the
+// descriptor word by word; the caller synchronises before and after.
+__device__ __forceinline__ void fft_load_box(const BatchDev &bt, int b, BoxDev &sb) {
+  static_assert(sizeof(BoxDev) % 8 == 0, "BoxDev is copied in 8-byte words");
+  for (int w = threadIdx.x; w < (int)(sizeof(BoxDev) / 8); w += FFT_T)
+    reinterpret_cast<unsigned long long *>(&sb)[w] =
+        __ldg(reinterpret_cast<const unsigned long long *>(bt.boxes + b) + w);
 }
 
 // ---------------------------------------------------------------------------
@@ -361,6 +381,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
   unsigned long long *bar = (unsigned long long *)(tws + sm.tw);
+  BoxDev &sb = *reinterpret_cast<BoxDev *>(bar + 2);   // descriptor of the box of the current tile
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -378,16 +399,20 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
     if (tn < total) {
       int ln;
       const int bn = tile_box(bt, tn, ln);
-      if (threadIdx.x == 0) fft_y_fwd_issue(bt.boxes[bn], ln, (double *)slot[(it + 1) & 1], &bar[(it + 1) & 1]);
-      fft_y_fwd_zero_tail(bt.boxes[bn], ln, (double *)slot[(it + 1) & 1]);
+      const BoxDev &Bn = bn == loaded ? sb : bt.boxes[bn];
+      if (threadIdx.x == 0) fft_y_fwd_issue(Bn, ln, (double *)slot[(it + 1) & 1], &bar[(it + 1) & 1]);
+      fft_y_fwd_zero_tail(Bn, ln, (double *)slot[(it + 1) & 1]);
     }
     const int b = tile_box(bt, t, lt);
-    const BoxDev &B = bt.boxes[b];
-    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
-    if (run && b != loaded) {
-      for (int q = threadIdx.x; q < B.nym; q += FFT_T) tws[q] = __ldg(B.twy + q);
+    if (b != loaded) {
+      __syncthreads();
+      fft_load_box(bt, b, sb);
+      __syncthreads();
+      for (int q = threadIdx.x; q < sb.nym; q += FFT_T) tws[q] = __ldg(sb.twy + q);
       loaded = b;
     }
+    const BoxDev &B = sb;
+    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
     const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
@@ -406,6 +431,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
                           NoDst{});
       // unpack the two real transforms: A = (Z_q + conj Z_{N-q}) / 2,
       // B = (Z_q - conj Z_{N-q}) / (2i)
+      double2 *const speck = B.spec + (long long)k * nzm * nh;
       for (int u = threadIdx.x; u < Pp * nh; u += FFT_T) {
         const int p = u & (Pp - 1), q = u >> lgP;
         const int i = i0 + 2 * p;
@@ -414,9 +440,9 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
         const double2 zn = cur[sidx(p, q == 0 ? 0 : N - q, lgP)];
         const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
         const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
-        const long long base = ((long long)k * nzm + i) * nh + q;
-        B.spec[base] = A;
-        if (i + 1 < nzm) B.spec[base + nh] = Bv;
+        const long long base = (long long)i * nh + q;
+        __stcg(speck + base, A);
+        if (i + 1 < nzm) __stcg(speck + base + nh, Bv);
       }
     }
     // the slot is refilled by bulk copies in the next iteration
@@ -436,7 +462,7 @@ struct ZDst {
   __device__ __forceinline__ void operator()(int l, int n, double2 v) const {
     const int ky = ky0 + l;
     if (ky >= nh) return;
-    spec[(long long)n * nh + ky] = v;
+    __stcg(spec + (long long)n * nh + ky, v);
   }
 };
 
@@ -460,6 +486,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
   unsigned long long *bar = (unsigned long long *)(tws + sm.tw);
+  BoxDev &sb = *reinterpret_cast<BoxDev *>(bar + 2);   // descriptor of the box of the current tile
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -476,15 +503,18 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
     if (tn < total && threadIdx.x == 0) {
       int ln;
       const int bn = tile_box(bt, tn, ln);
-      fft_z_issue(bt.boxes[bn], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
+      fft_z_issue(bn == loaded ? sb : bt.boxes[bn], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
     }
     const int b = tile_box(bt, t, lt);
-    const BoxDev &B = bt.boxes[b];
-    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
-    if (run && b != loaded) {
-      for (int q = threadIdx.x; q < B.nzm; q += FFT_T) tws[q] = __ldg(B.twz + q);
+    if (b != loaded) {
+      __syncthreads();
+      fft_load_box(bt, b, sb);
+      __syncthreads();
+      for (int q = threadIdx.x; q < sb.nzm; q += FFT_T) tws[q] = __ldg(sb.twz + q);
       loaded = b;
     }
+    const BoxDev &B = sb;
+    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
     const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       // a copy did not complete: flag the box, let the other slot's copy
@@ -659,8 +689,8 @@ struct YInvDst {
   double *phi; int N, nzm, i0;
   __device__ __forceinline__ void operator()(int p, int j, double2 v) const {
     const int i = i0 + 2 * p;
-    if (i < nzm) phi[(long long)i * N + j] = v.x;
-    if (i + 1 < nzm) phi[(long long)(i + 1) * N + j] = v.y;
+    if (i < nzm) __stcg(phi + (long long)i * N + j, v.x);
+    if (i + 1 < nzm) __stcg(phi + (long long)(i + 1) * N + j, v.y);
   }
 };
 
@@ -694,6 +724,7 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, Fft
   double2 *slot[2] = {fsm, fsm + sm.slot};
   double2 *tws = fsm + 2 * sm.slot;
   unsigned long long *bar = (unsigned long long *)(tws + sm.tw);
+  BoxDev &sb = *reinterpret_cast<BoxDev *>(bar + 2);   // descriptor of the box of the current tile
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -711,16 +742,20 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, Fft
     if (tn < total) {
       int ln;
       const int bn = tile_box(bt, tn, ln);
-      if (threadIdx.x == 0) fft_y_inv_issue(bt.boxes[bn], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
-      fft_y_inv_zero_tail(bt.boxes[bn], ln, slot[(it + 1) & 1]);
+      const BoxDev &Bn = bn == loaded ? sb : bt.boxes[bn];
+      if (threadIdx.x == 0) fft_y_inv_issue(Bn, ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
+      fft_y_inv_zero_tail(Bn, ln, slot[(it + 1) & 1]);
     }
     const int b = tile_box(bt, t, lt);
-    const BoxDev &B = bt.boxes[b];
-    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
-    if (run && b != loaded) {
-      for (int q = threadIdx.x; q < B.nym; q += FFT_T) tws[q] = __ldg(B.twy + q);
+    if (b != loaded) {
+      __syncthreads();
+      fft_load_box(bt, b, sb);
+      __syncthreads();
+      for (int q = threadIdx.x; q < sb.nym; q += FFT_T) tws[q] = __ldg(sb.twy + q);
       loaded = b;
     }
+    const BoxDev &B = sb;
+    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
     const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
