@@ -361,6 +361,10 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
     const int jj = (j0 + hj - 1 + nym) % nym, ii = (i0 + hi - 1 + nzm) % nzm;
     g[q] = (long long)ii * nym + jj;
   }
+  // source of this thread's per-k scalar (threads tid < K1_NTAB), resolved
+  // once: inside the march every descriptor read after a global store is a
+  // reload, and the 14 cases would diverge within the first warp each plane
+  const double *tsrc = tid < K1_NTAB ? k1_tab_src(B, tid, 0) : nullptr;
   auto load_plane = [&](int p) {      // plane p and its per-k scalars into slot p % NS
     if (p > nx - 1) return;
     const int sl = p % NS;
@@ -372,7 +376,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
       for (int q = 0; q < NLD; ++q)
         if (q * NT + tid < PL) cp_async8(dst + f * PL + tid + q * NT, fld[f] + po + g[q]);
     }
-    if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + sl * 16 + tid, k1_tab_src(B, tid, p));
+    if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + sl * 16 + tid, tsrc + p);
   };
   auto load_hist = [&](int p, double (&h)[4]) {
     if (inside && p <= nxm - 1) {
