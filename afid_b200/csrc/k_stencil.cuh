@@ -378,10 +378,16 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
     }
     if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + sl * 16 + tid, tsrc + p);
   };
+  // this column's history and forward-sweep outputs, resolved once (read
+  // from the descriptor inside the march, each would be reloaded after every
+  // global store, which might alias the descriptor)
+  double *const rux = B.rux + col, *const ruy = B.ruy + col, *const ruz = B.ruz + col, *const rut = B.rutemp + col;
+  double *const yb0 = B.ybuf[0] + col, *const yb1 = B.ybuf[1] + col, *const yb2 = B.ybuf[2] + col,
+                *const yb3 = B.ybuf[3] + col;
   auto load_hist = [&](int p, double (&h)[4]) {
     if (inside && p <= nxm - 1) {
-      const long long o = (long long)p * P + col;
-      h[0] = __ldcg(B.rux + o); h[1] = __ldcg(B.ruy + o); h[2] = __ldcg(B.ruz + o); h[3] = __ldcg(B.rutemp + o);
+      const long long o = (long long)p * P;
+      h[0] = __ldcg(rux + o); h[1] = __ldcg(ruy + o); h[2] = __ldcg(ruz + o); h[3] = __ldcg(rut + o);
     }
   };
 
@@ -422,7 +428,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
       acc.s_p = (kc + 1) % NS;
       const double *tk = tring + (kc % NS) * 16;
       if (inside) {
-        const long long o = (long long)kc * P + col;
+        const long long o = (long long)kc * P;
         const int dkm = kc == 0 ? 0 : -1;
         const int dkp = kc == nxm - 1 ? 0 : 1;
         const double udx3m_k = tk[KT_UDX3M];
@@ -433,20 +439,20 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
           const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
           const double r = rhs_vyz(H, hc[u][1], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
                                    acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
-          __stwb(B.ruy + o, H);
+          __stwb(ruy + o, H);
           const double bb = r * tk[KT_YSC];
           yY = (kc == 0) ? bb : bb - tk[KT_YF] * yY;
-          __stwb(B.ybuf[1] + o, yY);
+          __stwb(yb1 + o, yY);
         }
         {
           const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
           const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
           const double r = rhs_vyz(H, hc[u][2], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
                                    acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
-          __stwb(B.ruz + o, H);
+          __stwb(ruz + o, H);
           const double bb = r * tk[KT_YSC];
           yZ = (kc == 0) ? bb : bb - tk[KT_YF] * yZ;
-          __stwb(B.ybuf[2] + o, yZ);
+          __stwb(yb2 + o, yZ);
         }
         if (kc >= 1) {
           const double udx3c_k = tk[KT_UDX3C];
@@ -456,19 +462,19 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
             const double r = rhs_vx(H, hc[u][0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
                                     acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
                                     am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
-            __stwb(B.rux + o, H);
+            __stwb(rux + o, H);
             const double bb = r * tk[KT_XSC];
             yX = bb - tk[KT_XF] * yX;
-            __stwb(B.ybuf[0] + o, yX);
+            __stwb(yb0 + o, yX);
           }
           {
             const double H = h_temp(acc, c, udx3c_k);
             const double r = rhs_temp(H, hc[u][3], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
                                       acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
-            __stwb(B.rutemp + o, H);
+            __stwb(rut + o, H);
             const double bb = r * tk[KT_TSC];
             yT = bb - tk[KT_TF] * yT;
-            __stwb(B.ybuf[3] + o, yT);
+            __stwb(yb3 + o, yT);
           }
         }
         // stash what plane kc+1 will need of this plane
@@ -699,6 +705,7 @@ __global__ void __launch_bounds__(256, 2) k_divergence(BatchDev bt, int ns) {
   double *__restrict__ phi = B.phi + col;
   const double usdtal = 1.0 / (S->dt * S->al);
   const double dz = B.dz, dy = B.dy;
+  const double *__restrict__ t_udx3m = B.tab + (long long)T_UDX3M * B.nx;   // resolved before the stores
   double xk = vx[0];
   for (int k0 = 0; k0 < nxm; k0 += KD_U) {
     double zc[KD_U], zp[KD_U], yc[KD_U], yp[KD_U], xn[KD_U];
@@ -717,7 +724,7 @@ __global__ void __launch_bounds__(256, 2) k_divergence(BatchDev bt, int ns) {
       const int k = k0 + u;
       if (k >= nxm) break;
       // CalcLocalDivergence.F90:34-37
-      const double dq = (zp[u] - zc[u]) * dz + (yp[u] - yc[u]) * dy + (xn[u] - xk) * tabk(B, T_UDX3M, k);
+      const double dq = (zp[u] - zc[u]) * dz + (yp[u] - yc[u]) * dy + (xn[u] - xk) * __ldg(t_udx3m + k);
       phi[(long long)k * P] = dq * usdtal;
       xk = xn[u];
     }
