@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
 // sweep, q += dq), then the wall conditions of ImplicitAndUpdateVX.F90:76-77
 // and ImplicitAndUpdateTemp.F90:69-73.  One thread per column.
 // ---------------------------------------------------------------------------
-constexpr int K2_U = 4;   // planes loaded per chunk (loads of a chunk are all in flight together)
+constexpr int K2_U = 3;   // planes loaded per chunk (loads of a chunk are all in flight together; 4 spills at 80 registers)
 
 __global__ void __launch_bounds__(256, 3) k_implicit_bwd(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
@@ -513,13 +513,10 @@ __global__ void __launch_bounds__(256, 3) k_implicit_bwd(BatchDev bt, int ns) {
   if (col >= B.plane) return;
   const int nx = B.nx, nxm = B.nxm;
   const long long P = B.plane;
-  const double *__restrict__ dX = coefp(B, SYS_X, C_DP);
-  const double *__restrict__ uX = coefp(B, SYS_X, C_DU);
-  const double *__restrict__ dY = coefp(B, SYS_YZ, C_DP);
-  const double *__restrict__ uY = coefp(B, SYS_YZ, C_DU);
-  const double *__restrict__ dT = coefp(B, SYS_T, C_DP);
-  const double *__restrict__ uT = coefp(B, SYS_T, C_DU);
-  const double *__restrict__ gT = coefp(B, SYS_T, C_G);
+  // the LU rows of the three systems, as offsets from one base (seven
+  // separate pointers would hold 14 registers across both sweeps)
+  const double *__restrict__ cf = B.coef;
+  const auto lu = [&](int sys, int arr, int k) { return __ldg(cf + (long long)(sys * C_N + arr) * nx + k); };
   const double *__restrict__ y0 = B.ybuf[0] + col;
   const double *__restrict__ y1 = B.ybuf[1] + col;
   const double *__restrict__ y2 = B.ybuf[2] + col;
@@ -546,19 +543,19 @@ __global__ void __launch_bounds__(256, 3) k_implicit_bwd(BatchDev bt, int ns) {
       const int k = k0 - u;
       if (k < 0) break;
       const long long o = (long long)k * P;
-      const double dy_ = __ldg(dY + k);
+      const double dy_ = lu(SYS_YZ, C_DP, k);
       if (k == nxm - 1) {
         xY = a1[u] / dy_;
         xZ = a2[u] / dy_;
       } else {
-        const double uu = __ldg(uY + k);
+        const double uu = lu(SYS_YZ, C_DU, k);
         xY = (a1[u] - uu * xY) / dy_;
         xZ = (a2[u] - uu * xZ) / dy_;
       }
       vy[o] = q1[u] + xY;
       vz[o] = q2[u] + xZ;
       if (k >= 1) {
-        xX = (a0[u] - __ldg(uX + k) * xX) / __ldg(dX + k);
+        xX = (a0[u] - lu(SYS_X, C_DU, k) * xX) / lu(SYS_X, C_DP, k);
         vx[o] = q0[u] + xX;
       }
     }
@@ -580,8 +577,8 @@ __global__ void __launch_bounds__(256, 3) k_implicit_bwd(BatchDev bt, int ns) {
     for (int u = 0; u < K2_U; ++u) {
       const int k = k0 - u;
       if (k < 1) break;
-      const double y = a3[u] + __ldg(gT + k) * w;
-      xT = (y - __ldg(uT + k) * xT) / __ldg(dT + k);
+      const double y = a3[u] + lu(SYS_T, C_G, k) * w;
+      xT = (y - lu(SYS_T, C_DU, k) * xT) / lu(SYS_T, C_DP, k);
       tp[(long long)k * P] = q3[u] + xT;
     }
   }
