@@ -45,8 +45,8 @@ UNIT = "Mpoint-steps/s"
 # the number of cells, the kernels having the same per-cell structure at every
 # size.
 NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
-    "explicit_fwd": 135.4, "implicit_bwd": 95.1, "divergence": 36.4, "fft_y_fwd": 14.4,
-    "fft_z_fwd": 14.5, "poisson_x": 33.9, "fft_z_inv": 14.5, "fft_y_inv": 14.6, "diag": 32.4,
+    "explicit_fwd": 135.1, "implicit_bwd": 94.9, "divergence": 31.4, "fft_y_fwd": 14.3,
+    "fft_z_fwd": 14.3, "poisson_x": 30.3, "fft_z_inv": 14.4, "fft_y_inv": 14.5, "diag": 32.4,
 }
 
 
