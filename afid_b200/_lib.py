@@ -36,6 +36,7 @@ EXPORTS = [
     "afid_solve_pressure_correction_noalloc", "afid_box_set_tuning",
     "afid_global_quantities", "afid_calc_stats", "afid_calc_dissipation_nu", "afid_box_get_stats",
     "afid_box_reset_stats", "afid_slab_locations", "afid_slab_dump", "afid_box_set_time",
+    "afid_box_interp_field",
 ]
 
 STATS = ["vx_me", "vy_me", "vz_me", "temp_me", "vx_rms", "vy_rms", "vz_rms", "temp_rms", "tempvx_me",
@@ -129,6 +130,7 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_slab_locations": ([i, dp, dp, ip], i),
         "afid_slab_dump": ([vp, i, ip, i, dp], i),
         "afid_box_set_time": ([vp, i, d], i),
+        "afid_box_interp_field": ([vp, i, i, dp, i, i, i, i, d, i, d], i),
     }
     for name in ("explicit_terms_vx", "explicit_terms_vy", "explicit_terms_vz",
                  "explicit_terms_temp", "implicit_and_update_vx", "implicit_and_update_vy",

@@ -7,9 +7,9 @@ istr3 and str3.  ReadFlowField.F90 reads them back.  This image has no
 HDF5, so the same content is stored as raw little-endian FP64 files
 ``continua_<field>.bin`` (same element order as the HDF5 datasets) and a
 JSON master record ``continua_master.json`` with the same names.  A restart
-on the same grid restores the four fields and the time; the reference's
-interpolation onto a different grid (ReadFlowField.F90 with interp.F90) is
-not provided.
+on the same grid restores the four fields and the time; on another grid
+(ReadFlowField.F90:63-150) each field is interpolated onto the box's grid by
+the library (interp.F90), under the reference's conditions.
 """
 from __future__ import annotations
 
@@ -38,26 +38,40 @@ def write_fields(path: str, cfg, fields: dict, time: float) -> None:
         json.dump(master, fh, indent=1)
 
 
-def read_fields(path: str, cfg) -> tuple[dict, float]:
-    """Read the four fields (arrays a[k, j, i]) and the time; the grid of
-    the files must be the grid of ``cfg``."""
+def read_master(path: str) -> dict:
     with open(os.path.join(path, "continua_master.json")) as fh:
-        m = json.load(fh)
-    want = (cfg.nxm + 1, cfg.nym + 1, cfg.nzm + 1)
-    got = (m["nx"], m["ny"], m["nz"])
-    if got != want:
-        raise ValueError(f"continua grid (nx, ny, nz) = {got} differs from {want}: "
-                         "interpolation onto a new grid is not provided")
-    if m["istr3"] != cfg.istr3 or m["str3"] != cfg.str3:
-        raise ValueError("continua were written on another x grid (istr3/str3)")
-    shape = (cfg.nxm + 1, cfg.nym, cfg.nzm)
+        return json.load(fh)
+
+
+def same_grid(m: dict, cfg) -> bool:
+    """ReadFlowField.F90:75-77: no interpolation when nx, ny, nz and istr3
+    match and str3 differs by at most 1e-8."""
+    return (m["ny"] == cfg.nym + 1 and m["nx"] == cfg.nxm + 1 and m["nz"] == cfg.nzm + 1
+            and m["istr3"] == cfg.istr3 and not abs(m["str3"] - cfg.str3) > 1e-8)
+
+
+def read_raw(path: str, m: dict) -> dict:
+    """The four datasets of continua files with master record ``m``, as
+    arrays a[k, j, i] of shape (nx, ny-1, nz-1) of the files' grid."""
+    shape = (m["nx"], m["ny"] - 1, m["nz"] - 1)
     out = {}
     for name in FIELDS:
         a = np.fromfile(os.path.join(path, f"continua_{name}.bin"), dtype="<f8")
         if a.size != np.prod(shape):
             raise ValueError(f"continua_{name}.bin holds {a.size} values, expected {np.prod(shape)}")
         out[name] = a.reshape(shape, order="F")
-    return out, float(m["time"])
+    return out
+
+
+def read_fields(path: str, cfg) -> tuple[dict, float]:
+    """Read the four fields (arrays a[k, j, i]) and the time; the grid of
+    the files must be the grid of ``cfg``."""
+    m = read_master(path)
+    if not same_grid(m, cfg):
+        raise ValueError(f"continua grid (nx, ny, nz, istr3, str3) = "
+                         f"{(m['nx'], m['ny'], m['nz'], m['istr3'], m['str3'])} differs from the box's: "
+                         "use read_flow_field, which interpolates")
+    return read_raw(path, m), float(m["time"])
 
 
 def write_flow_field(box, path: str) -> None:
@@ -66,10 +80,17 @@ def write_flow_field(box, path: str) -> None:
 
 
 def read_flow_field(box, path: str) -> float:
-    """ReadFlowField on the same grid: upload the four fields, set the time;
-    returns the time."""
-    fields, time = read_fields(path, box.cfg)
-    for name, a in fields.items():
-        box.upload(name, a)
-    box.set_time(time)
-    return time
+    """ReadFlowField: the four fields onto the box (uploaded as they are on
+    the same grid, interpolated on the device onto the box's grid
+    otherwise), then the time; returns the time."""
+    m = read_master(path)
+    fields = read_raw(path, m)
+    if same_grid(m, box.cfg):
+        for name, a in fields.items():
+            box.upload(name, a)
+    else:
+        # ReadFlowField.F90:102-150 regrids vz, vy, vx, temp in that order
+        for name in ("vz", "vy", "vx", "temp"):
+            box.interp_field(name, fields[name], m["nx"], m["ny"], m["nz"], m["istr3"], m["str3"])
+    box.set_time(float(m["time"]))
+    return float(m["time"])

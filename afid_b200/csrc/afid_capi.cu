@@ -961,6 +961,95 @@ int afid_box_set_time(afid_ctx *c, int id, double time) {
   return 0;
 }
 
+// ---- restart onto a new grid (ReadFlowField.F90:63-150, interp.F90) ------
+// gridnew (interp.F90:229-296): nodes rc and centres rm of an n-point grid on
+// [0, rext] for istr 0 and 6 (for those, CreateGrid's nodes), indexed 0..n+1
+// with the second-order extrapolated ends of interp.F90:45-60
+static int gridnew_pad(int n, double rext, int istr, double stri, std::vector<double> &rc, std::vector<double> &rm) {
+  rc.assign(n + 2, 0.0);
+  rm.assign(n + 2, 0.0);
+  if (afid_make_grid(n - 1, istr, stri, rext, rc.data() + 1)) return -1;
+  for (int i = 1; i < n; ++i) rm[i] = (rc[i] + rc[i + 1]) * 0.5;
+  rm[n] = 2 * rc[n] - rm[n - 1];
+  for (std::vector<double> *v : {&rc, &rm}) {
+    std::vector<double> &a = *v;
+    a[0] = 2 * a[1] - a[2];
+    a[n + 1] = 2 * a[n] - a[n - 1];
+  }
+  return 0;
+}
+
+// per new coordinate: the new value, the bracketing old values and indices
+// (interp.F90:128-175), as five rows of length m at t
+static void interp_axis(const std::vector<double> &oldc, int n, const std::vector<double> &newc, int m, double *t) {
+  for (int q = 0; q < m; ++q) {
+    const double b = newc[q + 1];
+    int f = n - 1, cc = n;
+    for (int l = 1; l <= n; ++l)
+      if (oldc[l] >= b) { f = l - 1; cc = l; break; }
+    t[q] = b; t[m + q] = oldc[f]; t[2 * m + q] = oldc[cc]; t[3 * m + q] = f; t[4 * m + q] = cc;
+  }
+}
+
+int afid_box_interp_field(afid_ctx *c, int id, int field, const double *old, int nxo, int nyo, int nzo,
+                          int istro3, double stro3, int istr3, double str3) {
+  if (!c || !old) return fail(AFID_EINVAL, "interp_field: null argument");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  // interp.F90's case per field as ReadFlowField.F90:70-73 numbers them
+  // (vxflag = 1 ... teflag = 4); case 1 is staggered in z and case 3 in x
+  int flag;
+  switch (field) {
+    case AFID_VX: flag = 1; break;
+    case AFID_VY: flag = 2; break;
+    case AFID_VZ: flag = 3; break;
+    case AFID_TEMP: flag = 4; break;
+    default: return fail(AFID_EINVAL, "interp_field: field must be vx, vy, vz or temp");
+  }
+  const afid_box_params &p = hb->prm;
+  const int nx = p.nxm + 1, ny = p.nym + 1, nz = p.nzm + 1;
+  if (nz > nzo * 2 || ny > nyo * 2 || nx > nxo * 2)   // ReadFlowField.F90:88-99
+    return fail(AFID_EINVAL, "interp_field: new grid resolution cannot be more than twice the old resolution");
+  if (nxo < 3 || nyo < 3 || nzo < 3) return fail(AFID_EINVAL, "interp_field: old grid too small (nx, ny, nz >= 3)");
+  if ((istro3 != 0 && istro3 != 6) || (istr3 != 0 && istr3 != 6))
+    return fail(AFID_EINVAL, "interp_field: interp.F90's gridnew defines istr3 0 and 6 only (got %d, %d)", istro3, istr3);
+  std::vector<double> tco, tmo, rco, rmo, zzo, zmo, tcn, tmn, rcn, rmn, zzn, zmn;
+  if (gridnew_pad(nzo, p.zlen, 0, 1.0, tco, tmo) || gridnew_pad(nyo, p.ylen, 0, 1.0, rco, rmo) ||
+      gridnew_pad(nxo, 1.0, istro3, stro3, zzo, zmo) || gridnew_pad(nz, p.zlen, 0, 1.0, tcn, tmn) ||
+      gridnew_pad(ny, p.ylen, 0, 1.0, rcn, rmn) || gridnew_pad(nx, 1.0, istr3, str3, zzn, zmn))
+    return fail(AFID_EINVAL, "interp_field: grid construction failed");
+  const std::vector<double> &xo = flag == 1 ? tco : tmo, &xn = flag == 1 ? tcn : tmn;
+  const std::vector<double> &yo = flag == 2 ? rco : rmo, &yn = flag == 2 ? rcn : rmn;
+  const std::vector<double> &zo = flag == 3 ? zzo : zmo, &zn = flag == 3 ? zzn : zmn;
+  const int nzm = p.nzm, nym = p.nym, nyom = nyo - 1, nzom = nzo - 1;
+  const size_t ntab = 5 * ((size_t)nzm + nym + nx), nold = (size_t)nxo * nyom * nzom;
+  std::vector<double> tab(ntab);
+  interp_axis(xo, nzo, xn, nzm, tab.data());
+  interp_axis(yo, nyo, yn, nym, tab.data() + 5 * (size_t)nzm);
+  interp_axis(zo, nxo, zn, nx, tab.data() + 5 * ((size_t)nzm + nym));
+  rc = set_device(c);
+  if (rc) return rc;
+  double *buf = nullptr;
+  if (cudaMalloc(&buf, (ntab + nold) * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(AFID_ENOMEM, "interp_field: %zu bytes of device memory", (ntab + nold) * sizeof(double));
+  }
+  const BoxDev &d = hb->dev;
+  double *dst = field == AFID_VX ? d.vx : field == AFID_VY ? d.vy : field == AFID_VZ ? d.vz : d.temp;
+  const long long npt = (long long)nx * nym * nzm;
+  cudaStream_t st = c->stream;
+  bool ok = cudaMemcpyAsync(buf, tab.data(), ntab * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(buf + ntab, old, nold * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess;
+  if (ok) {
+    k_interp<<<(unsigned)((npt + 255) / 256), 256, 0, st>>>(buf + ntab, nxo, nyom, nzom, buf, dst, nx, nym, nzm);
+    ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  cudaFree(buf);
+  if (!ok) return fail(AFID_ECUDA, "interp_field: copy or kernel failed");
+  return 0;
+}
+
 int afid_box_get_scalars(afid_ctx *c, int id, afid_box_scalars *out) {
   if (!c || !out) return fail(AFID_EINVAL, "null argument");
   HostBox *hb;

@@ -139,4 +139,65 @@ __global__ void __launch_bounds__(256) k_implicit_one(const BoxDev *__restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// Restart onto a new grid (ReadFlowField.F90:63-150, interp.F90:11-227): one
+// thread per point of the new grid, written in the device layout.  The old
+// field a(1:nxo, 1:nyom, 1:nzom) is the continua dataset in Fortran order;
+// its halo is extrapolated on the fly as interp.F90:95-117 fills it, on the
+// six faces only (edges and corners, which the reference never writes, are
+// zero).  ``tab`` holds per new point of each direction (z: nzm, then y: nym,
+// then x: nx entries) the new coordinate, the two bracketing old
+// coordinates and their indices (interp.F90:128-175), each as a row of the
+// direction's length.  The stencil and the operation order are those of
+// interp.F90:177-227 and interptrilin, including the three upper-x corners
+// read at the lower x index (sffc, sccc, scfc).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double interp_old(const double *__restrict__ a, int nxo, int nyom, int nzom,
+                                             int k, int j, int i) {
+  const int hx = (k == 0 || k == nxo + 1), hy = (j == 0 || j == nyom + 1), hz = (i == 0 || i == nzom + 1);
+  const auto A = [&](int kk, int jj, int ii) {
+    return __ldg(a + (kk - 1) + (long long)nxo * ((jj - 1) + (long long)nyom * (ii - 1)));
+  };
+  if (hx + hy + hz == 0) return A(k, j, i);
+  if (hx + hy + hz > 1) return 0.0;
+  if (hx) return k == 0 ? 2.0 * A(1, j, i) - A(2, j, i) : 2.0 * A(nxo, j, i) - A(nxo - 1, j, i);
+  if (hz) return i == 0 ? 2.0 * A(k, j, 1) - A(k, j, 2) : 2.0 * A(k, j, nzom) - A(k, j, nzom - 1);
+  return j == 0 ? 2.0 * A(k, 1, i) - A(k, 2, i) : 2.0 * A(k, nyom, i) - A(k, nyom - 1, i);
+}
+
+__global__ void __launch_bounds__(256) k_interp(const double *__restrict__ a, int nxo, int nyom, int nzom,
+                                                const double *__restrict__ tab, double *__restrict__ out,
+                                                int nx, int nym, int nzm) {
+  const long long plane = (long long)nym * nzm;
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)nx * plane) return;
+  const int k = (int)(q / plane);
+  const long long r = q - (long long)k * plane;
+  const int i = (int)(r / nym), j = (int)(r - (long long)i * nym);
+  const double *tx = tab, *ty = tab + 5LL * nzm, *tz = ty + 5LL * nym;
+  const double bix = tx[i], bix1 = tx[nzm + i], bix2 = tx[2 * nzm + i];
+  const int fi = (int)tx[3 * nzm + i], ci = (int)tx[4 * nzm + i];
+  const double biy = ty[j], biy1 = ty[nym + j], biy2 = ty[2 * nym + j];
+  const int fj = (int)ty[3 * nym + j], cj = (int)ty[4 * nym + j];
+  const double biz = tz[k], biz1 = tz[nx + k], biz2 = tz[2 * nx + k];
+  const int fk = (int)tz[3 * nx + k], ck = (int)tz[4 * nx + k];
+  const double aficjfk = interp_old(a, nxo, nyom, nzom, fk, cj, fi);
+  const double afifjfk = interp_old(a, nxo, nyom, nzom, fk, fj, fi);
+  const double acicjfk = interp_old(a, nxo, nyom, nzom, fk, cj, ci);
+  const double acifjfk = interp_old(a, nxo, nyom, nzom, fk, fj, ci);
+  const double aficjck = interp_old(a, nxo, nyom, nzom, ck, cj, fi);
+  const double afifjck = afifjfk;   // sffc = arrold(bifk, bifj, bifi)
+  const double acicjck = acicjfk;   // sccc = arrold(bifk, bicj, bici)
+  const double acifjck = acifjfk;   // scfc = arrold(bifk, bifj, bici)
+  const double dxdydz = 1.0 / ((bix2 - bix1) * (biy2 - biy1) * (biz2 - biz1));
+  out[q] = (aficjfk * (bix2 - bix) * (biy - biy1) * (biz2 - biz)
+            + afifjfk * (bix2 - bix) * (biy2 - biy) * (biz2 - biz)
+            + acicjfk * (bix - bix1) * (biy - biy1) * (biz2 - biz)
+            + acifjfk * (bix - bix1) * (biy2 - biy) * (biz2 - biz)
+            + aficjck * (bix2 - bix) * (biy - biy1) * (biz - biz1)
+            + afifjck * (bix2 - bix) * (biy2 - biy) * (biz - biz1)
+            + acicjck * (bix - bix1) * (biy - biy1) * (biz - biz1)
+            + acifjck * (bix - bix1) * (biy2 - biy) * (biz - biz1)) * dxdydz;
+}
+
 }  // namespace afid

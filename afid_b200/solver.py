@@ -187,6 +187,20 @@ class Box:
         """Simulation time of the box (as restored from continua files)."""
         _lib.check(self._L.afid_box_set_time(self.ctx.h, self.id, float(time)))
 
+    def interp_field(self, field: str, old: np.ndarray, nxo: int, nyo: int, nzo: int,
+                     istro3: int, stro3: float):
+        """One continua dataset of a run on another grid (nxo, nyo, nzo points,
+        wall-normal grid istro3/stro3), interpolated onto this box's grid on
+        the device as ReadFlowField.F90:63-150 / interp.F90 do.  ``old`` is
+        a[k, j, i] of shape (nxo, nyo-1, nzo-1)."""
+        a = np.asarray(old, dtype=np.float64)
+        if a.shape != (nxo, nyo - 1, nzo - 1):
+            raise ValueError(f"old field shape {a.shape}, expected {(nxo, nyo - 1, nzo - 1)}")
+        buf = np.ascontiguousarray(a.ravel(order="F"))
+        _lib.check(self._L.afid_box_interp_field(self.ctx.h, self.id, _lib.FIELDS[field], _lib.dptr(buf),
+                                                 nxo, nyo, nzo, int(istro3), float(stro3),
+                                                 int(self.cfg.istr3), float(self.cfg.str3)))
+
     def reset(self, dt: float = 0.0):
         _lib.check(self._L.afid_box_reset(self.ctx.h, self.id, dt))
 

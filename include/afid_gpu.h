@@ -130,6 +130,21 @@ int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
 /* Set the simulation time (the time a restart reads from the continua
  * master record, ReadFlowField.F90:24-40). */
 int afid_box_set_time(afid_ctx *ctx, int box_id, double time);
+/* Restart onto a new grid (ReadFlowField.F90:63-150 with interp.F90:11-227):
+ * ``old`` is one continua dataset (nxo x (nyo-1) x (nzo-1) values in Fortran
+ * order, x fastest) of a run with nxo, nyo, nzo points and wall-normal grid
+ * istro3/stro3; it is interpolated onto this box's grid (wall-normal grid
+ * istr3/str3) and written into ``field`` (AFID_VX, AFID_VY, AFID_VZ or
+ * AFID_TEMP) on the device.  As in the reference: at most twice the old
+ * points in each direction, istr3 0 or 6 for both grids (the only ones
+ * interp.F90's gridnew defines), x grids of extent 1, the field numbering
+ * of ReadFlowField (vx regridded on interp's case 1, staggered in z; vz on
+ * case 3, staggered in x), faces of the old halo extrapolated linearly,
+ * and the stencil of interp.F90:177-191 with three upper-x corners read at
+ * the lower x index.  The halo's edges and corners, unset in the
+ * reference, are zero.  Allocates a temporary device buffer. */
+int afid_box_interp_field(afid_ctx *ctx, int box_id, int field, const double *old, int nxo, int nyo, int nzo,
+                          int istro3, double stro3, int istr3, double str3);
 int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
 /* Launch-shape tuning of one box (no counterpart in the reference):
  * row pairs per y-FFT block and ky columns per z-FFT block (powers of two;

@@ -996,3 +996,131 @@ def run(s: State, nsteps: int, dt: float, idtv: int = 0, cflmax: float = 1.2,
         recs.append(dict(ntime=ntime, dt=dt, cfl=cfl_used, err=err,
                          nu_bot=nub, nu_top=nut, div=check_divergence(s)))
     return recs
+
+
+# ----------------------------------------------------------------------------
+# Restart onto a new grid: ReadFlowField.F90:63-150 with interp.F90:11-227
+# ----------------------------------------------------------------------------
+# interp.F90's case selector per field, as ReadFlowField.F90:70-73 passes it
+# (vxflag = 1 ... teflag = 4).  Case 1 interpolates on the z nodes and case 3
+# on the x nodes (interp.F90:65-94), so vx is regridded with vz's staggering
+# and vz with vx's: the reference's behaviour, kept.
+INTERP_FLAG = {"vx": 1, "vy": 2, "vz": 3, "temp": 4}
+
+
+def gridnew(n: int, rext: float, istr: int, stri: float) -> tuple[np.ndarray, np.ndarray]:
+    """interp.F90:229-296 with the halo extrapolation of interp.F90:45-60:
+    nodes rc and centres rm of an n-point grid on [0, rext], as arrays indexed
+    like the Fortran ones, 0..n+1 (rc(0), rc(n+1), rm(0), rm(n+1) extrapolated
+    to second order).  gridnew defines istr 0 (uniform) and 6 (clipped
+    Chebyshev) only; for those its nodes are CreateGrid's."""
+    if istr not in (0, 6):
+        raise ValueError(f"interp.F90's gridnew defines istr 0 and 6 only (got {istr})")
+    rc = np.zeros(n + 2)
+    rm = np.zeros(n + 2)
+    rc[1:n + 1] = make_xc(n - 1, istr, stri, rext)
+    for i in range(1, n):
+        rm[i] = (rc[i] + rc[i + 1]) * 0.5
+    rm[n] = 2 * rc[n] - rm[n - 1]
+    for a in (rc, rm):
+        a[0] = 2 * a[1] - a[2]
+        a[n + 1] = 2 * a[n] - a[n - 1]
+    return rc, rm
+
+
+def interp_check(nxo: int, nyo: int, nzo: int, istro3: int, nx: int, ny: int, nz: int, istr3: int) -> None:
+    """The conditions ReadFlowField.F90:88-99 and interp.F90's gridnew put
+    on a regrid (point counts nx = nxm + 1, ny = nym + 1, nz = nzm + 1)."""
+    if nz > nzo * 2 or ny > nyo * 2 or nx > nxo * 2:
+        raise ValueError("new grid resolution cannot be more than twice the old resolution")
+    if min(nxo, nyo, nzo) < 3:
+        raise ValueError("old grid too small to extrapolate its halo")
+    for s in (istro3, istr3):
+        if s not in (0, 6):
+            raise ValueError(f"interp.F90's gridnew defines istr 0 and 6 only (got {s})")
+
+
+def _bracket(old: np.ndarray, n: int, new: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """interp.F90:137-169: for each new coordinate the first old index l in
+    1..n with old(l) >= new, returned as (l-1, l); (n-1, n) when there is none."""
+    ge = old[None, 1:n + 1] >= new[:, None]
+    has = ge.any(axis=1)
+    l = np.where(has, ge.argmax(axis=1) + 1, n)
+    return np.where(has, l - 1, n - 1), l
+
+
+def interp_field(old: np.ndarray, nxo: int, nyo: int, nzo: int, istro3: int, stro3: float,
+                 flag: int, nxm: int, nym: int, nzm: int, istr3: int, str3: float,
+                 ylen: float, zlen: float) -> np.ndarray:
+    """One field of a snapshot interpolated onto the grid (nxm, nym, nzm)
+    (interp.F90:11-227).  ``old`` is a[k, j, i] of shape (nxo, nyo-1, nzo-1)
+    (the continua dataset); the result has shape (nxm+1, nym, nzm).
+
+    As in the reference: the old array's halo is filled by linear
+    extrapolation on its six faces only (interp.F90:95-117); the stencil
+    reads the lower x index in three of its four upper-x corners
+    (interp.F90:184-191, sffc/sccc/scfc); the x grids are built with
+    extent 1 whatever alx3 (interp.F90:42,64).  The halo's edges and corners,
+    which the reference never writes yet reads for new points below the
+    first old point in two directions, are zero here (what a fresh
+    allocation holds)."""
+    nx, ny, nz = nxm + 1, nym + 1, nzm + 1
+    interp_check(nxo, nyo, nzo, istro3, nx, ny, nz, istr3)
+    nyom, nzom = nyo - 1, nzo - 1
+    if old.shape != (nxo, nyom, nzom):
+        raise ValueError(f"old field shape {old.shape}, expected {(nxo, nyom, nzom)}")
+    tco, tmo = gridnew(nzo, zlen, 0, 1.0)
+    rco, rmo = gridnew(nyo, ylen, 0, 1.0)
+    zzo, zmo = gridnew(nxo, 1.0, istro3, stro3)
+    tcn, tmn = gridnew(nz, zlen, 0, 1.0)
+    rcn, rmn = gridnew(ny, ylen, 0, 1.0)
+    zzn, zmn = gridnew(nx, 1.0, istr3, str3)
+    xold, yold, zold, xnew, ynew, znew = {
+        1: (tco, rmo, zmo, tcn, rmn, zmn),
+        2: (tmo, rco, zmo, tmn, rcn, zmn),
+        3: (tmo, rmo, zzo, tmn, rmn, zzn),
+        4: (tmo, rmo, zmo, tmn, rmn, zmn)}[flag]
+    # padded old array a(0:nxo+1, 0:nyom+1, 0:nzom+1)
+    a = np.zeros((nxo + 2, nyom + 2, nzom + 2))
+    a[1:nxo + 1, 1:nyom + 1, 1:nzom + 1] = old
+    a[0, 1:nyom + 1, 1:nzom + 1] = 2.0 * a[1, 1:nyom + 1, 1:nzom + 1] - a[2, 1:nyom + 1, 1:nzom + 1]
+    a[nxo + 1, 1:nyom + 1, 1:nzom + 1] = 2.0 * a[nxo, 1:nyom + 1, 1:nzom + 1] - a[nxo - 1, 1:nyom + 1, 1:nzom + 1]
+    a[1:nxo + 1, 1:nyom + 1, 0] = 2.0 * a[1:nxo + 1, 1:nyom + 1, 1] - a[1:nxo + 1, 1:nyom + 1, 2]
+    a[1:nxo + 1, 1:nyom + 1, nzom + 1] = 2.0 * a[1:nxo + 1, 1:nyom + 1, nzom] - a[1:nxo + 1, 1:nyom + 1, nzom - 1]
+    a[1:nxo + 1, 0, 1:nzom + 1] = 2.0 * a[1:nxo + 1, 1, 1:nzom + 1] - a[1:nxo + 1, 2, 1:nzom + 1]
+    a[1:nxo + 1, nyom + 1, 1:nzom + 1] = 2.0 * a[1:nxo + 1, nyom, 1:nzom + 1] - a[1:nxo + 1, nyom - 1, 1:nzom + 1]
+    # interp's x, y, z are the z, y, x directions: i (nzm), j (nym), k (nx)
+    bix = xnew[1:nzm + 1]
+    biy = ynew[1:nym + 1]
+    biz = znew[1:nx + 1]
+    fi, ci = _bracket(xold, nzo, bix)
+    fj, cj = _bracket(yold, nyo, biy)
+    fk, ck = _bracket(zold, nxo, biz)
+    bix1, bix2 = xold[fi], xold[ci]
+    biy1, biy2 = yold[fj], yold[cj]
+    biz1, biz2 = zold[fk], zold[ck]
+    K = (slice(None), None, None)
+    J = (None, slice(None), None)
+    I = (None, None, slice(None))
+    FK, CK, FJ, CJ, FI, CI = fk[K], ck[K], fj[J], cj[J], fi[I], ci[I]
+    aficjfk = a[FK, CJ, FI]
+    afifjfk = a[FK, FJ, FI]
+    acicjfk = a[FK, CJ, CI]
+    acifjfk = a[FK, FJ, CI]
+    aficjck = a[CK, CJ, FI]
+    afifjck = a[FK, FJ, FI]
+    acicjck = a[FK, CJ, CI]
+    acifjck = a[FK, FJ, CI]
+    X, X1, X2 = bix[I], bix1[I], bix2[I]
+    Y, Y1, Y2 = biy[J], biy1[J], biy2[J]
+    Z, Z1, Z2 = biz[K], biz1[K], biz2[K]
+    dxdydz = 1.0 / ((X2 - X1) * (Y2 - Y1) * (Z2 - Z1))
+    ans = (aficjfk * (X2 - X) * (Y - Y1) * (Z2 - Z)
+           + afifjfk * (X2 - X) * (Y2 - Y) * (Z2 - Z)
+           + acicjfk * (X - X1) * (Y - Y1) * (Z2 - Z)
+           + acifjfk * (X - X1) * (Y2 - Y) * (Z2 - Z)
+           + aficjck * (X2 - X) * (Y - Y1) * (Z - Z1)
+           + afifjck * (X2 - X) * (Y2 - Y) * (Z - Z1)
+           + acicjck * (X - X1) * (Y - Y1) * (Z - Z1)
+           + acifjck * (X - X1) * (Y2 - Y) * (Z - Z1)) * dxdydz
+    return np.ascontiguousarray(ans)
