@@ -103,7 +103,8 @@ int factor_radices(int n, int *rad, int *np) {
 // Variants of the explicit/forward kernel: tile height TI (block of 32 TI
 // threads), resident blocks per SM and planes per barrier.
 //   2: 32x8 tiles, 2 blocks/SM        3: 32x8 tiles, 3 blocks/SM (80 registers)
-//   4: 32x8 tiles, two planes per barrier
+//   4: 32x8 tiles, two planes per barrier (a 7-plane ring of 150 KB: one
+//      block per SM at 128 registers)
 //   5: 32x4 tiles, 4 blocks/SM        6: 32x2 tiles, 8 blocks/SM
 //   7: 32x4 tiles, 5 blocks/SM        8: 32x4 tiles, 6 blocks/SM
 constexpr int K1_VMIN = 2, K1_VMAX = 8;

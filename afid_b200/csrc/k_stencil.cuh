@@ -301,11 +301,12 @@ __device__ __forceinline__ const double *k1_tab_src(const BoxDev &B, int t, int 
 // and LU scalars, fetched with cp.async 2 PPB + 1 planes ahead so that each
 // load has two barrier intervals of compute to arrive in.  Plane k-1 is not
 // read from the ring: the seven values of it that the stencils need are kept
-// in registers.  The RK history of the next PPB planes is loaded into
-// registers one interval ahead.  Global loads and stores use the global
-// state space explicitly (ld.global / st.global intrinsics), so the compiler
-// knows they cannot touch the shared ring and keeps stencil values in
-// registers across them.  Writes the RK history (rux.. = H) and the
+// in registers.  The RK history (the tile's own columns of rux, ruy, ruz,
+// rutemp) travels in the same ring as aligned 16-byte pairs, so no global
+// load of the march is waited for in registers.  Global stores use the global
+// state space explicitly (st.global intrinsics), so the compiler knows they
+// cannot touch the shared ring and keeps stencil values in registers across
+// them.  Writes the RK history (rux.. = H) and the
 // forward-sweep values y of each solve; the temperature sweep starts from
 // y(1) = 0 and the missing contribution of its wall row is added by K2 (the
 // solve is linear in y(1)).
@@ -314,7 +315,8 @@ template <int PPB, int TI = 8>
 struct K1Ring {
   static constexpr int D = 2 * PPB + 1;        // prefetch distance in planes
   static constexpr int NS = D + PPB;           // ring slots
-  static constexpr int SMEM = (NS * F_NF * K1Shape<TI>::PL + NS * 16) * 8;
+  static constexpr int HS = 4 * K1Shape<TI>::NT; // RK history of one plane (tile interior, 4 fields)
+  static constexpr int SMEM = (NS * F_NF * K1Shape<TI>::PL + NS * 16 + NS * HS) * 8;
 };
 
 template <int TI, int MINB, int PPB>
@@ -322,9 +324,11 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
   constexpr int NS = K1Ring<PPB, TI>::NS;
   constexpr int D = K1Ring<PPB, TI>::D;
   constexpr int PL = K1Shape<TI>::PL, NT = K1Shape<TI>::NT, NLD = K1Shape<TI>::NLD;
+  constexpr int HS = K1Ring<PPB, TI>::HS;
   extern __shared__ double k1sm[];
   double *ring = k1sm;
   double *tring = k1sm + NS * F_NF * PL;         // [slot][16]
+  double *hring = tring + NS * 16;               // [slot][field][NT], the column of thread t at t
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
@@ -365,6 +369,23 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
   // once: inside the march every descriptor read after a global store is a
   // reload, and the 14 cases would diverge within the first warp each plane
   const double *tsrc = tid < K1_NTAB ? k1_tab_src(B, tid, 0) : nullptr;
+  // the RK history of a plane travels with it in the ring: 4 fields x NT
+  // columns as 2 NT aligned 16-byte pairs, two per thread.  Pair r = tid +
+  // q NT is field r / (NT/2), tile row c / 16 and columns 2 (c % 16) + {0, 1}
+  // with c = r % (NT/2); a pair is inside the box or wholly outside it (j0
+  // and nym are even)
+  const double *hsrc[2];
+  int hdst[2];
+  bool hok[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int r = tid + q * NT, fq = r / (NT / 2), cc = r - fq * (NT / 2);
+    const int hrow = cc / 16, hj = 2 * (cc % 16);
+    const double *base = fq == 0 ? B.rux : fq == 1 ? B.ruy : fq == 2 ? B.ruz : B.rutemp;
+    hok[q] = (i0 + hrow < nzm) && (j0 + hj < nym);
+    hsrc[q] = base + (long long)(i0 + hrow) * nym + j0 + hj;
+    hdst[q] = fq * NT + hrow * K1_TJ + hj;
+  }
   auto load_plane = [&](int p) {      // plane p and its per-k scalars into slot p % NS
     if (p > nx - 1) return;
     const int sl = p % NS;
@@ -377,6 +398,9 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
         if (q * NT + tid < PL) cp_async8(dst + f * PL + tid + q * NT, fld[f] + po + g[q]);
     }
     if (tid < K1_NTAB && p <= nxm - 1) cp_async8(tring + sl * 16 + tid, tsrc + p);
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      if (hok[q] && p <= nxm - 1) cp_async16(hring + sl * HS + hdst[q], hsrc[q] + (long long)p * P);
   };
   // this column's history and forward-sweep outputs, resolved once (read
   // from the descriptor inside the march, each would be reloaded after every
@@ -384,12 +408,6 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
   double *const rux = B.rux + col, *const ruy = B.ruy + col, *const ruz = B.ruz + col, *const rut = B.rutemp + col;
   double *const yb0 = B.ybuf[0] + col, *const yb1 = B.ybuf[1] + col, *const yb2 = B.ybuf[2] + col,
                 *const yb3 = B.ybuf[3] + col;
-  auto load_hist = [&](int p, double (&h)[4]) {
-    if (inside && p <= nxm - 1) {
-      const long long o = (long long)p * P;
-      h[0] = __ldcg(rux + o); h[1] = __ldcg(ruy + o); h[2] = __ldcg(ruz + o); h[3] = __ldcg(rut + o);
-    }
-  };
 
   RingAcc<PL> acc;
   acc.ring = ring;
@@ -399,18 +417,11 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
   // forward-sweep carries
   double yX = inside ? B.wall[col] : 0.0;   // rhs(1,j,i) left by the last vz solve
   double yY = 0.0, yZ = 0.0, yT = 0.0;
-  double hc[PPB][4], hn[PPB][4];
-#pragma unroll
-  for (int u = 0; u < PPB; ++u)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) { hc[u][q] = 0.0; hn[u][q] = 0.0; }
 
   for (int p = 0; p < D - PPB; ++p) load_plane(p);
   cp_async_commit();
   for (int p = D - PPB; p < D; ++p) load_plane(p);
   cp_async_commit();
-#pragma unroll
-  for (int u = 0; u < PPB; ++u) load_hist(u, hc[u]);
   cp_async_wait_1();
   __syncthreads();
 
@@ -419,14 +430,13 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
     for (int u = 0; u < PPB; ++u) load_plane(k0 + D + u);
     cp_async_commit();
 #pragma unroll
-    for (int u = 0; u < PPB; ++u) load_hist(k0 + PPB + u, hn[u]);
-#pragma unroll
     for (int u = 0; u < PPB; ++u) {
       const int kc = k0 + u;
       if (kc >= nxm) break;
       acc.s_c = kc % NS;
       acc.s_p = (kc + 1) % NS;
       const double *tk = tring + (kc % NS) * 16;
+      const double *hk = hring + (kc % NS) * HS + tid;   // this column's history, field f at hk[f NT]
       if (inside) {
         const long long o = (long long)kc * P;
         const int dkm = kc == 0 ? 0 : -1;
@@ -437,7 +447,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
         {
           const double H = h_vy(acc, c, udx3m_k, dkm, dkp);
           const double dyp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, -1, 0)) * udy_al;
-          const double r = rhs_vyz(H, hc[u][1], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
+          const double r = rhs_vyz(H, hk[1 * NT], acc(F_VY, dkp, 0, 0), acc(F_VY, 0, 0, 0),
                                    acc(F_VY, dkm, 0, 0), am_s, ac_s, ap_s, dyp, ga, ro, alre, dt);
           __stwb(ruy + o, H);
           const double bb = r * tk[KT_YSC];
@@ -447,7 +457,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
         {
           const double H = h_vz(acc, c, udx3m_k, dkm, dkp);
           const double dzp = (acc(F_PR, 0, 0, 0) - acc(F_PR, 0, 0, -1)) * dz_ * al;
-          const double r = rhs_vyz(H, hc[u][2], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
+          const double r = rhs_vyz(H, hk[2 * NT], acc(F_VZ, dkp, 0, 0), acc(F_VZ, 0, 0, 0),
                                    acc(F_VZ, dkm, 0, 0), am_s, ac_s, ap_s, dzp, ga, ro, alre, dt);
           __stwb(ruz + o, H);
           const double bb = r * tk[KT_YSC];
@@ -459,7 +469,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
           const double am_c = tk[KT_AM3CK], ac_c = tk[KT_AC3CK], ap_c = tk[KT_AP3CK];
           {
             const double H = h_vx(acc, c, udx3c_k);
-            const double r = rhs_vx(H, hc[u][0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
+            const double r = rhs_vx(H, hk[0], acc(F_VX, 1, 0, 0), acc(F_VX, 0, 0, 0),
                                     acc(F_VX, -1, 0, 0), acc(F_PR, 0, 0, 0), acc(F_PR, -1, 0, 0),
                                     am_c, ac_c, ap_c, al, ga, ro, alre, dt, udx3c_k);
             __stwb(rux + o, H);
@@ -469,7 +479,7 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
           }
           {
             const double H = h_temp(acc, c, udx3c_k);
-            const double r = rhs_temp(H, hc[u][3], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
+            const double r = rhs_temp(H, hk[3 * NT], acc(F_T, 1, 0, 0), acc(F_T, 0, 0, 0),
                                       acc(F_T, -1, 0, 0), am_c, ac_c, ap_c, ga, ro, alpec, dt);
             __stwb(rut + o, H);
             const double bb = r * tk[KT_TSC];
@@ -487,10 +497,6 @@ __global__ void __launch_bounds__(K1Shape<TI>::NT, MINB) k_explicit_implicit_fwd
         acc.prev.pr = acc(F_PR, 0, 0, 0);
       }
     }
-#pragma unroll
-    for (int u = 0; u < PPB; ++u)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) hc[u][q] = hn[u][q];
     cp_async_wait_1();
     __syncthreads();
   }
