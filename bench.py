@@ -45,7 +45,7 @@ UNIT = "Mpoint-steps/s"
 # the number of cells, the kernels having the same per-cell structure at every
 # size.
 NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
-    "explicit_fwd": 135.1, "implicit_bwd": 94.9, "divergence": 31.4, "fft_y_fwd": 14.3,
+    "explicit_fwd": 135.5, "implicit_bwd": 94.9, "divergence": 31.4, "fft_y_fwd": 14.3,
     "fft_z_fwd": 14.3, "poisson_x": 30.3, "fft_z_inv": 14.4, "fft_y_inv": 14.5, "diag": 32.4,
 }
 
