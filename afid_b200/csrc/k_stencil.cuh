@@ -145,7 +145,7 @@ __global__ void k_substep_prep(const BoxDev *__restrict__ boxes, int nbox, int n
   if (!B.active || ns >= B.nsst) return;
   BoxScalars *S = B.sc;
   if (S->status != 0) return;
-  __shared__ double s_al, s_beta, s_bx[3];
+  __shared__ double s_bx[3];
   if (threadIdx.x == 0) {
     double gam[3], rom[3];
     if (B.nsst > 1) {
@@ -159,7 +159,6 @@ __global__ void k_substep_prep(const BoxDev *__restrict__ boxes, int nbox, int n
     const double al = gam[ns] + rom[ns];
     const double beta = dt / B.ren * 0.5;     // TimeMarcher.F90:22
     S->al = al; S->ga = gam[ns]; S->ro = rom[ns]; S->beta = beta;
-    s_al = al; s_beta = beta;
     s_bx[SYS_X] = beta * al;
     s_bx[SYS_YZ] = beta * al;
     s_bx[SYS_T] = 0.5 * al * dt / B.pec;     // SolveImpEqnUpdate_Temp.F90:25
