@@ -75,7 +75,7 @@ struct Batch {
   int k2_block = 256;               // threads per block of the back-substitution kernel
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
-  int k1_minb = 2;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
+  int k1_minb = 4;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
 };
 
 long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
@@ -108,6 +108,7 @@ int factor_radices(int n, int *rad, int *np) {
 //   5: 32x4 tiles, 4 blocks/SM        6: 32x2 tiles, 8 blocks/SM
 //   7: 32x4 tiles, 5 blocks/SM        8: 32x4 tiles, 6 blocks/SM
 constexpr int K1_VMIN = 2, K1_VMAX = 8;
+constexpr int K1_DEFAULT = 4;   // the variant the tuner picks for the large boxes (768^2, 1280^2)
 int k1_tile_height(int variant) { return (variant == 5 || variant >= 7) ? 4 : variant == 6 ? 2 : 8; }
 
 long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 256) {
@@ -416,8 +417,8 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     // one variant of the explicit/forward kernel per launch: the one the
     // boxes holding most of the cells ask for
     long long w[K1_VMAX + 1] = {};
-    for (const BoxDev &d : devs) w[d.k1_minb >= K1_VMIN && d.k1_minb <= K1_VMAX ? d.k1_minb : 2] += d.fsize;
-    bt->k1_minb = 2;
+    for (const BoxDev &d : devs) w[d.k1_minb >= K1_VMIN && d.k1_minb <= K1_VMAX ? d.k1_minb : K1_DEFAULT] += d.fsize;
+    bt->k1_minb = K1_DEFAULT;
     for (int v = K1_VMIN; v <= K1_VMAX; ++v)
       if (w[v] > w[bt->k1_minb]) bt->k1_minb = v;
     const char *e = getenv("AFID_K1_VARIANT");
@@ -772,7 +773,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   d.pec = std::sqrt(p->pra * p->ray);
   d.tempbp = p->tempbp; d.temptp = p->temptp;
   d.hist_cap = HIST_CAP;
-  d.k1_minb = 2;
+  d.k1_minb = K1_DEFAULT;
   const size_t fb = 9 * (size_t)s.fsize * sizeof(double);
   const size_t sb = (size_t)(s.scratch + s.nspec) * sizeof(double);   // + the Poisson pivot table
   const size_t mb = (size_t)s.small * sizeof(double);
@@ -1108,7 +1109,7 @@ int afid_box_set_tuning(afid_ctx *c, int id, int fft_y_lines, int fft_z_lines, i
   CK(cudaStreamSynchronize(c->stream));
   d.fy_lines = fft_y_lines;
   d.fz_lines = fft_z_lines;
-  d.k1_minb = k1_minb ? k1_minb : 2;
+  d.k1_minb = k1_minb ? k1_minb : K1_DEFAULT;
   rc = write_z_map(d, c->stream);   // the TMA box width follows the z lines
   if (rc) return rc;
   // batches hold copies of the descriptor and tile tables: drop them

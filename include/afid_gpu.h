@@ -151,7 +151,7 @@ int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
  * 0 = built-in choice) and the variant of the explicit/forward kernel:
  * 2 = 32x8-column tiles, two resident blocks per SM; 3 = 32x8, three
  * resident blocks; 4 = 32x8, two planes per barrier; 5, 7, 8 = 32x4 tiles,
- * four, five or six blocks; 6 = 32x2 tiles, eight blocks (0 = 2).  Results
+ * four, five or six blocks; 6 = 32x2 tiles, eight blocks (0 = 4).  Results
  * do not depend on these values. */
 int afid_box_set_tuning(afid_ctx *ctx, int box_id, int fft_y_lines, int fft_z_lines, int k1_minb);
 /* Copies up to max_records of the most recent per-step records, oldest
