@@ -9,6 +9,9 @@ golden_c1_nu.npz  box 65x64x64, Ra=1e6, Pr=1, dt=5e-4, seed 0 (the plain
                   single-box configuration): per-step plate Nusselt numbers,
                   dt and max divergence for 100 steps, plus per-field
                   checksums (sum, sum of squares) after 100 steps.
+golden_c1_seeds.npz  the same box for seeds 0, 1 and 2: per-step plate
+                  Nusselt numbers and dt of the first 100 steps
+                  (keys s<seed>_nu_bot, s<seed>_nu_top, s<seed>_dt).
 The Fortran reference cannot be compiled here, so these vectors pin the
 oracle against itself across changes (regression) and pin the CUDA path
 against the oracle; the oracle is pinned to the reference's formulas by the
@@ -63,7 +66,24 @@ def c1(nsteps=100):
     np.savez_compressed(os.path.join(HERE, "golden_c1_nu.npz"), **out)
 
 
+def c1_seeds(seeds=(0, 1, 2), nsteps=100):
+    cfg = cfg_of(**C1)
+    out = {}
+    for seed in seeds:
+        s = oracle_state(cfg, seed=seed)
+        recs = O.run(s, nsteps, cfg.dt, vectorised_poisson=True)
+        out[f"s{seed}_nu_bot"] = np.array([r["nu_bot"] for r in recs])
+        out[f"s{seed}_nu_top"] = np.array([r["nu_top"] for r in recs])
+        out[f"s{seed}_dt"] = np.array([r["dt"] for r in recs])
+    np.savez_compressed(os.path.join(HERE, "golden_c1_seeds.npz"), **out)
+
+
 if __name__ == "__main__":
-    small()
-    c1()
+    which = sys.argv[1:] or ["small", "c1", "c1_seeds"]
+    if "small" in which:
+        small()
+    if "c1" in which:
+        c1()
+    if "c1_seeds" in which:
+        c1_seeds()
     print("golden fixtures written")
