@@ -14,6 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafid_gpu.so")
 
 AFID_OK = 0
+STATUS_HELD = 1          # afid_box_scalars.status of a box on hold (not an error)
+STATUS_DEVICE_TIMEOUT = 990   # a transform's tile copy did not complete within the wait limit
 ERRORS = {-1: "AFID_EINVAL", -2: "AFID_ENOMEM", -3: "AFID_ECUDA", -4: "AFID_ENOBOX",
           -5: "AFID_EFFT", -6: "AFID_ESIZE"}
 
@@ -36,7 +38,8 @@ EXPORTS = [
     "afid_solve_pressure_correction_noalloc", "afid_box_set_tuning",
     "afid_global_quantities", "afid_calc_stats", "afid_calc_dissipation_nu", "afid_box_get_stats",
     "afid_box_reset_stats", "afid_slab_locations", "afid_slab_dump", "afid_box_set_time",
-    "afid_box_interp_field",
+    "afid_box_interp_field", "afid_box_set_stop", "afid_box_resume",
+    "afid_box_test_skip_z_copies",
 ]
 
 STATS = ["vx_me", "vy_me", "vz_me", "temp_me", "vx_rms", "vy_rms", "vz_rms", "temp_rms", "tempvx_me",
@@ -120,7 +123,7 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_step": ([vp, ip, i, i], i), "afid_step_graph": ([vp, ip, i, i], i),
         "afid_substep": ([vp, ip, i, i], i),
         "afid_step_profiled": ([vp, ip, i, i, dp, ip, i], i),
-        "afid_solve_pressure_correction_noalloc": ([vp, i, i, i, dp, d, d, d, vp], i),
+        "afid_solve_pressure_correction_noalloc": ([vp, i, i, i, dp, d, d, d, vp, ip], i),
         "afid_box_set_tuning": ([vp, i, i, i, i], i),
         "afid_global_quantities": ([vp, i, C.POINTER(GlobalQ)], i),
         "afid_calc_stats": ([vp, i], i),
@@ -131,6 +134,8 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_slab_dump": ([vp, i, ip, i, dp], i),
         "afid_box_set_time": ([vp, i, d], i),
         "afid_box_interp_field": ([vp, i, i, dp, i, i, i, i, d, i, d], i),
+        "afid_box_set_stop": ([vp, i, i, d, d], i), "afid_box_resume": ([vp, i], i),
+        "afid_box_test_skip_z_copies": ([vp, i, i, C.c_uint], i),
     }
     for name in ("explicit_terms_vx", "explicit_terms_vy", "explicit_terms_vz",
                  "explicit_terms_temp", "implicit_and_update_vx", "implicit_and_update_vy",

@@ -61,8 +61,8 @@ def fft_z_bytes(n: int, lines: int) -> int:
 
 
 def candidates(cfg: BouIn) -> dict:
-    ny = [v for v in (1, 2, 4, 8, 16) if fft_y_bytes(cfg.nym, v) <= SMEM_MAX and v * cfg.nym <= TILE_MAX]
-    nz = [v for v in (1, 2, 4, 8, 16) if fft_z_bytes(cfg.nzm, v) <= SMEM_MAX and v * cfg.nzm <= TILE_MAX
+    ny = [v for v in (1, 2, 4, 8, 16, 32, 64) if fft_y_bytes(cfg.nym, v) <= SMEM_MAX and v * cfg.nym <= TILE_MAX]
+    nz = [v for v in (1, 2, 4, 8, 16, 32, 64) if fft_z_bytes(cfg.nzm, v) <= SMEM_MAX and v * cfg.nzm <= TILE_MAX
           and v < 2 * (cfg.nym // 2 + 1)]
     return {"fft_y_lines": ny or [1], "fft_z_lines": nz or [1], "k1_minb": [2, 3, 4, 5, 6, 7, 8]}
 

@@ -47,6 +47,7 @@ int fail(int code, const char *fmt, ...) {
       return fail(AFID_ECUDA, "launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
+// Launch families; each has its own table of tile offsets per batch.
 enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, FAM_K2, NFAM };
 constexpr int HIST_CAP = 4096;
 
@@ -120,13 +121,13 @@ long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 
     case FAM_DIAG: return cdiv(B.plane, 256);
     case FAM_FY: return (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
     case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
-    case FAM_PX: return cdiv((long long)B.nzm * B.nymh, 256);
+    case FAM_PX: return cdiv(px_pairs(B.nzm, B.nymh), 256);
   }
   return 0;
 }
 
 struct Sizes {
-  long long nx, plane, fsize, nspec, scratch, small;
+  long long nx, plane, fsize, nspec, npiv, scratch, small;
 };
 
 Sizes sizes_of(const afid_box_params &p) {
@@ -135,6 +136,7 @@ Sizes sizes_of(const afid_box_params &p) {
   s.plane = (long long)p.nym * p.nzm;
   s.fsize = s.nx * s.plane;
   s.nspec = (long long)p.nxm * p.nzm * (p.nym / 2 + 1);
+  s.npiv = (long long)p.nxm * px_pairs(p.nzm, p.nym / 2 + 1);   // pivot table: kz <= nzm/2
   long long pois = 3 * s.nspec + 1 + (long long)p.nxm * s.plane;   // dph 16-byte aligned
   s.scratch = pois > 4 * s.fsize ? pois : 4 * s.fsize;
   // tables + twiddles + coef + nu partials + history + scalars (in doubles)
@@ -338,6 +340,7 @@ int get_box(afid_ctx *c, int id, HostBox **out) {
 
 int init_kernel_attrs();
 
+
 // slot sizes (complex values) and twiddle lengths of the persistent
 // transforms, grown to cover box d
 void fft_smem_grow(const BoxDev &d, FftSmem &y, FftSmem &z, int &twy, int &twz) {
@@ -513,6 +516,17 @@ struct Prof {
     }                               \
   } while (0)
 
+// The x-solve of the Poisson equation (total[f] tiles of family f; bd(f)
+// its descriptor).
+template <class BD>
+int launch_poisson_x(const int *total, BD bd, cudaStream_t s, int ns) {
+  if (total[FAM_PX] > 0) {
+    k_poisson_x<<<total[FAM_PX], 256, 0, s>>>(bd(FAM_PX), ns);
+    CKL();
+  }
+  return 0;
+}
+
 int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof *pf = nullptr) {
   if (from_vel) {
     k_divergence<<<bt->total[FAM_COL], 256, 0, s>>>(bdev(bt, FAM_COL), ns);
@@ -525,8 +539,10 @@ int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof 
   k_fft_z<-1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
   PMARK(pf, AFID_K_FFT_Z_FWD);
-  k_poisson_x<<<bt->total[FAM_PX], 256, 0, s>>>(bdev(bt, FAM_PX), ns);
-  CKL();
+  {
+    int rc = launch_poisson_x(bt->total, [&](int fam) { return bdev(bt, fam); }, s, ns);
+    if (rc) return rc;
+  }
   PMARK(pf, AFID_K_POISSON_X);
   k_fft_z<+1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
@@ -740,7 +756,7 @@ int afid_make_grid(int nxm, int istr3, double str3, double alx3, double *xc) {
 size_t afid_box_device_bytes(const afid_box_params *p) {
   if (!p) return 0;
   Sizes s = sizes_of(*p);
-  return (size_t)(9 * s.fsize + s.scratch + s.nspec + s.small) * sizeof(double) + 2 * sizeof(BoxDev) + 4096;
+  return (size_t)(9 * s.fsize + s.scratch + s.npiv + s.small) * sizeof(double) + 2 * sizeof(BoxDev) + 4096;
 }
 
 int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *box_id) {
@@ -775,7 +791,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
   d.hist_cap = HIST_CAP;
   d.k1_minb = K1_DEFAULT;
   const size_t fb = 9 * (size_t)s.fsize * sizeof(double);
-  const size_t sb = (size_t)(s.scratch + s.nspec) * sizeof(double);   // + the Poisson pivot table
+  const size_t sb = (size_t)(s.scratch + s.npiv) * sizeof(double);   // + the Poisson pivot table
   const size_t mb = (size_t)s.small * sizeof(double);
   if (cudaMalloc(&hb->mem_fields, fb) != cudaSuccess || cudaMalloc(&hb->mem_scratch, sb) != cudaSuccess ||
       cudaMalloc(&hb->mem_small, mb) != cudaSuccess || cudaMalloc(&hb->d_self, sizeof(BoxDev)) != cudaSuccess) {
@@ -830,8 +846,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
             cudaMemcpyAsync((void *)d.twy, tw.data(), tw.size() * 16, cudaMemcpyHostToDevice, st) == cudaSuccess &&
             cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st) == cudaSuccess;
   if (ok) {   // the Poisson pivots depend on the grid only: tabulate them once
-    const long long nmode = (long long)p->nzm * d.nymh;
-    k_poisson_pivots<<<(unsigned)((nmode + 255) / 256), 256, 0, st>>>(d);
+    k_poisson_pivots<<<(unsigned)cdiv(px_pairs(p->nzm, d.nymh), 256), 256, 0, st>>>(d);
     ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess;
     d.piv_ready = 1;
   }
@@ -1066,6 +1081,56 @@ int afid_box_get_scalars(afid_ctx *c, int id, afid_box_scalars *out) {
   out->divmax = bs.divmax;
   for (int q = 0; q < 3; ++q) out->vmax[q] = bs.vmax[q];
   out->nu_bot = bs.nu_bot; out->nu_top = bs.nu_top; out->ntime = bs.ntime; out->status = bs.status;
+  return 0;
+}
+
+int afid_box_set_stop(afid_ctx *c, int id, int stop_ntime, double tout, double tmax) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  static_assert(AFID_STATUS_HELD == AFID_STATUS_HELD_DEV, "hold status of the C-ABI and the kernels");
+  const int stop = stop_ntime > 0 ? stop_ntime : 0;
+  const double to = tout > 0 ? tout : 0.0, tm = tmax > 0 ? tmax : 0.0;
+  char *sc = (char *)hb->dev.sc;
+  CK(cudaMemcpyAsync(sc + offsetof(BoxScalars, stop_ntime), &stop, sizeof stop, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(sc + offsetof(BoxScalars, tout), &to, sizeof to, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(sc + offsetof(BoxScalars, tmax), &tm, sizeof tm, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int afid_box_test_skip_z_copies(afid_ctx *c, int id, int skip, unsigned max_polls) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  hb->dev.z_copy_skip = skip ? 1 : 0;
+  hb->dev.mbar_tries = max_polls;
+  // batches hold copies of the descriptor: drop the ones with this box
+  for (auto it = c->batches.begin(); it != c->batches.end();) {
+    bool has = false;
+    for (int x : it->first) has |= (x == id);
+    if (has) { free_batch(it->second); it = c->batches.erase(it); }
+    else ++it;
+  }
+  return sync_self(hb);
+}
+
+int afid_box_resume(afid_ctx *c, int id) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  HostBox *hb;
+  int rc = get_box(c, id, &hb);
+  if (rc) return rc;
+  rc = set_device(c);
+  if (rc) return rc;
+  k_resume<<<1, 32, 0, c->stream>>>(hb->d_self, 1);
+  CKL();
   return 0;
 }
 
@@ -1564,9 +1629,12 @@ extern "C" int afid_slab_dump(afid_ctx *c, int id, const int *kslab, int nslab, 
 // The array is fixed at AFID_NOALLOC_DOUBLES doubles (about 48.5 MiB) and
 // every GPU on which the library is loaded holds it until the process exits.
 // Every call shares it and it keeps the previous call's contents; each call
-// rewrites everything it reads, so nothing has to start at zero.  Calls
-// whose work overlaps on the GPU (two streams, or two host threads) race on
-// it and must be serialised by the caller.
+// rewrites everything it reads (the status word is cleared by each call),
+// so nothing has to start at zero.  Calls whose work overlaps on the GPU
+// (two streams, or two host threads) race on it and must be serialised by
+// the caller.  A call stages its small per-call data (tables, descriptor,
+// status word) through host memory that the next call reuses, so a call on
+// a stream that is being captured into a graph is refused.
 // ============================================================================
 namespace {
 
@@ -1605,8 +1673,19 @@ NoallocHost g_noalloc_host;
 
 extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int nym, int nzm,
                                                       const double *xc, double alx3, double ylen,
-                                                      double zlen, void *stream) {
+                                                      double zlen, void *stream, int *status) {
   if (!dph || !xc) return fail(AFID_EINVAL, "noalloc: dph and xc are required");
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t e = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(AFID_EINVAL, "noalloc: the stream's capture state cannot be read (%s)", cudaGetErrorString(e));
+    }
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(AFID_EINVAL, "noalloc: the stream is being captured; this entry point stages per-call data "
+                               "through host memory and cannot be recorded into a graph");
+  }
   if (nxm < 3 || nym < 2 || nzm < 2 || (nym % 2))
     return fail(AFID_EINVAL, "noalloc: need nxm >= 3, nzm >= 2 and an even nym >= 2");
   if (!(alx3 > 0) || !(ylen > 0) || !(zlen > 0)) return fail(AFID_EINVAL, "noalloc: lengths must be > 0");
@@ -1698,14 +1777,19 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   d.sc = (BoxScalars *)(base + o_sc);
   d.tm_z = (const CUtensorMap *)(base + o_tm);
   d.active = 1;
+  d.piv_ready = 1;   // k_poisson_pivots runs first in every call
   rc = encode_z_map(d, &g_noalloc_host.tm);
   if (rc) return rc;
   BoxScalars bs;
   memset(&bs, 0, sizeof bs);
-  int off[3][2];
-  off[0][0] = 0; off[0][1] = (int)tiles_of(d, FAM_FY);
-  off[1][0] = 0; off[1][1] = (int)tiles_of(d, FAM_FZ);
-  off[2][0] = 0; off[2][1] = (int)tiles_of(d, FAM_PX);
+  // one-box tile tables of every family (only the transforms' and the
+  // x-solve's are used)
+  int off[NFAM][2], total[NFAM];
+  static_assert(sizeof(off) <= 16 * sizeof(double), "tile tables exceed their scratch slot");
+  for (int f = 0; f < NFAM; ++f) {
+    off[f][0] = 0;
+    off[f][1] = total[f] = (f == FAM_FY || f == FAM_FZ || f == FAM_PX) ? (int)tiles_of(d, f) : 0;
+  }
   CK(cudaMemcpyAsync(base + o_tab, tab, (size_t)n_tab * 8, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_tw, g_noalloc_host.tw, (size_t)(nym + nzm) * 16, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st));
@@ -1714,24 +1798,35 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   CK(cudaMemcpyAsync(base + o_tm, &g_noalloc_host.tm, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
   const BoxDev *dbox = (const BoxDev *)(base + o_box);
   const int *doff = (const int *)(base + o_off);
-  BatchDev fy{dbox, doff + 0, 1}, fz{dbox, doff + 2, 1}, px{dbox, doff + 4, 1};
+  auto bd = [&](int fam) { return BatchDev{dbox, doff + 2 * fam, 1}; };
   FftSmem smy{0, 0}, smz{0, 0};
   int twy = 0, twz = 0, gy = 0, gz = 0;
   fft_smem_grow(d, smy, smz, twy, twz);
   const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + FFT_TAIL_BYTES;
   const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + FFT_TAIL_BYTES;
-  rc = fft_grid(k_fft_y_fwd, sy, off[0][1], &gy);
-  if (!rc) rc = fft_grid(k_fft_z<-1>, sz, off[1][1], &gz);
+  rc = fft_grid(k_fft_y_fwd, sy, total[FAM_FY], &gy);
+  if (!rc) rc = fft_grid(k_fft_z<-1>, sz, total[FAM_FZ], &gz);
   if (rc) return rc;
-  k_fft_y_fwd<<<gy, FFT_T, sy, st>>>(fy, 0, smy, off[0][1]);
+  // the x-solve's pivots, for this call's grid
+  k_poisson_pivots<<<(unsigned)cdiv(px_pairs(nzm, d.nymh), 256), 256, 0, st>>>(d);
   CKL();
-  k_fft_z<-1><<<gz, FFT_T, sz, st>>>(fz, 0, smz, off[1][1]);
+  k_fft_y_fwd<<<gy, FFT_T, sy, st>>>(bd(FAM_FY), 0, smy, total[FAM_FY]);
   CKL();
-  k_poisson_x<<<off[2][1], 256, 0, st>>>(px, 0);
+  k_fft_z<-1><<<gz, FFT_T, sz, st>>>(bd(FAM_FZ), 0, smz, total[FAM_FZ]);
   CKL();
-  k_fft_z<+1><<<gz, FFT_T, sz, st>>>(fz, 0, smz, off[1][1]);
+  rc = launch_poisson_x(total, bd, st, 0);
+  if (rc) return rc;
+  k_fft_z<+1><<<gz, FFT_T, sz, st>>>(bd(FAM_FZ), 0, smz, total[FAM_FZ]);
   CKL();
-  k_fft_y_inv<<<gy, FFT_T, sy, st>>>(fy, 0, smy, off[0][1]);
+  k_fft_y_inv<<<gy, FFT_T, sy, st>>>(bd(FAM_FY), 0, smy, total[FAM_FY]);
   CKL();
+  if (status) {
+    // wait for this call's kernels and report its status word
+    int v = -1;
+    CK(cudaMemcpyAsync(&v, (char *)(base + o_sc) + offsetof(BoxScalars, status), sizeof v,
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *status = v;
+  }
   return 0;
 }

@@ -36,7 +36,18 @@ struct BoxScalars {
   int nonfinite;    // set when a non-finite value is seen by the diagnostics
   unsigned long long red_u64[4];  // atomicMax scratch: cfl, div, vmax_y, vmax_z
   double nu_partial_dummy;
+  // holds (afid_box_set_stop): after a step the box is put on hold (status
+  // AFID_STATUS_HELD) when ntime reaches stop_ntime (> 0), with tout > 0 at
+  // an output time of main.F90:207 (second step, or mod(time, tout) < dt),
+  // and with tmax > 0 once time > tmax (main.F90:256)
+  double tout;
+  double tmax;
+  int stop_ntime;
+  int pad_hold_;
 };
+
+// status of a box on hold: skipped like a failed box until resumed
+constexpr int AFID_STATUS_HELD_DEV = 1;
 
 // Offsets of the metric tables inside BoxDev::tab (length nx each unless
 // noted).  Index k is 0-based (k = kc-1 of the reference).
@@ -75,8 +86,8 @@ struct BoxDev {
   // Poisson scratch (aliases ybuf storage; live only between the divergence
   // and the correction)
   double2 *spec;        // [k][kz][ky], k < nxm, ky <= nym/2
-  double *dstore;       // Thomas pivots of the Poisson solve, same indexing
-                        // (a table of its own when piv_ready, else scratch)
+  double *dstore;       // reciprocal Thomas pivots 1/d of the Poisson solve,
+                        // same indexing (tabulated by k_poisson_pivots)
   double *phi;          // pressure correction dph, [k][i][j], k < nxm
   // reference-boundary mode buffers (allocated on first use)
   double *qcap, *dq, *hro, *rhs;
@@ -99,7 +110,12 @@ struct BoxDev {
   int fz_lines;         // tuning: ky columns per z-FFT block (0 = default)
   int fz_rb;            // kz rows per TMA box of the z transform (a divisor of nzm, <= 256)
   const CUtensorMap *tm_z;  // TMA map of spec as a 2-D FP64 array (2*nymh x nxm*nzm), box 2L x fz_rb
-  int piv_ready;        // 1 = dstore holds the Poisson pivots of this grid (tabulated once)
+  int piv_ready;        // 1 = dstore holds the Poisson pivots of this grid
+  // test switch of the bounded waits (afid_box_test_skip_z_copies): the z
+  // transform arms its slot mbarriers without issuing the box's tile copies,
+  // and its waits give up after mbar_tries polls (0: MBAR_MAX_TRIES)
+  int z_copy_skip;
+  unsigned mbar_tries;
 };
 
 // Work decomposition: each kernel family launches a 1-D grid over the
@@ -194,8 +210,9 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
-  for (unsigned t = 0; t < MBAR_MAX_TRIES; ++t)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity,
+                                                  unsigned tries = MBAR_MAX_TRIES) {
+  for (unsigned t = 0; t < tries; ++t)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

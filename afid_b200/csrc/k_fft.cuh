@@ -264,15 +264,16 @@ __device__ void fft_tile(double2 *a, int N, int lgL, const int *rad, int np, con
 }
 
 // Persistent transform blocks.  A launch has at most (SMs x resident blocks)
-// blocks; each takes tiles blockIdx.x, blockIdx.x + gridDim.x, ... and
-// copies the next tile into its second shared-memory slot (cp.async) while
-// it transforms the current one in place.  Shared memory: two slots and the
+// blocks; each takes runs of tiles (TileRange) and copies the next tile into
+// its second shared-memory slot (bulk copy or TMA) while it transforms the
+// current one in place.  Shared memory: two slots and the
 // twiddles of the box being transformed.  Lines per tile default to what
 // keeps two blocks on an SM (and at most FFT_TILE_MAX values per tile); the
 // tuning fields may choose other values within those limits.
 constexpr int FFT_SMEM_DEFAULT = 110 * 1024;
 constexpr int FFT_SMEM_MAX = 200 * 1024;
-constexpr int FFT_MAX_LINES = 16;
+constexpr int FFT_MAX_LINES = 64;      // lines per tile the tuning may ask for
+constexpr int FFT_DEFAULT_LINES = 16;  // and the built-in choice at most
 
 // y: a slot holds the 2 Pp real rows of a forward tile (Pp N complex) or the
 // 2 Pp half-spectrum rows of an inverse tile (2 Pp (N/2+1) complex)
@@ -288,13 +289,13 @@ __host__ __device__ __forceinline__ int fft_y_bytes(int N, int Pp) { return (2 *
 __host__ __device__ __forceinline__ int fft_z_bytes(int N, int L) { return (2 * L * N + N) * 16 + FFT_TAIL_BYTES; }
 __host__ __device__ __forceinline__ bool fft_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
 __host__ __device__ __forceinline__ bool fft_y_ok(int N, int Pp, int budget) {
-  return fft_pow2(Pp) && Pp * N <= FFT_TILE_MAX && fft_y_bytes(N, Pp) <= budget;
+  return fft_pow2(Pp) && Pp <= FFT_MAX_LINES && Pp * N <= FFT_TILE_MAX && fft_y_bytes(N, Pp) <= budget;
 }
 __host__ __device__ __forceinline__ bool fft_z_ok(int N, int L, int budget) {
-  return fft_pow2(L) && L * N <= FFT_TILE_MAX && fft_z_bytes(N, L) <= budget;
+  return fft_pow2(L) && L <= FFT_MAX_LINES && L * N <= FFT_TILE_MAX && fft_z_bytes(N, L) <= budget;
 }
 __host__ __device__ __forceinline__ int fft_fit_lines(int N, int budget, bool y) {
-  int l = FFT_MAX_LINES;
+  int l = FFT_DEFAULT_LINES;
   while (l > 1 && !(y ? fft_y_ok(N, l, budget) : fft_z_ok(N, l, budget))) l >>= 1;
   return l;
 }
@@ -305,7 +306,9 @@ __host__ __device__ __forceinline__ int ilog2(int v) {
 }
 __host__ __device__ __forceinline__ int fft_y_pairs(const BoxDev &B) {
   if (B.fy_lines > 0) return B.fy_lines;
-  return fft_fit_lines(B.nym, FFT_SMEM_DEFAULT, true);
+  int l = fft_fit_lines(B.nym, FFT_SMEM_DEFAULT, true);
+  while (l > 1 && l >= B.nzm) l >>= 1;        // no tile taller than needed
+  return l;
 }
 __host__ __device__ __forceinline__ int fft_z_lines(const BoxDev &B) {
   int l = B.fz_lines > 0 ? B.fz_lines : fft_fit_lines(B.nzm, FFT_SMEM_DEFAULT, false);
@@ -319,11 +322,39 @@ struct FftSmem {
   int tw;     // complex values of the twiddle table (the z transform's mbarriers follow it)
 };
 
-__device__ __forceinline__ int tile_box(const BatchDev &bt, int tile, int &local) {
-  const int b = find_box(bt.tile_off, bt.nbox, tile);
-  local = tile - __ldg(bt.tile_off + b);
-  return b;
-}
+// A persistent block takes runs of FFT_TILE_RUN consecutive tiles, the runs
+// dealt round-robin over the blocks (block p: runs p, p + G, p + 2G, ...):
+// neighbouring blocks work on neighbouring tiles at the same time, the work
+// of boxes of different sizes spreads over all blocks, and a block changes
+// boxes at most once per run.  A walker follows the tiles' boxes forward.
+constexpr int FFT_TILE_RUN = 4;
+struct TileRange {
+  int t0, total;
+  __device__ __forceinline__ explicit TileRange(int total_) : t0(blockIdx.x * FFT_TILE_RUN), total(total_) {}
+  __device__ __forceinline__ int first() const { return t0 < total ? t0 : total; }
+  __device__ __forceinline__ int next(int t) const {
+    int n = t + 1;
+    if (n % FFT_TILE_RUN == 0) n = (t / FFT_TILE_RUN + (int)gridDim.x) * FFT_TILE_RUN;
+    return n < total ? n : total;
+  }
+};
+struct TileWalk {
+  int b, lo, hi;   // box b holds the tiles [lo, hi) of the launch
+  __device__ __forceinline__ TileWalk(const BatchDev &bt, int t) {
+    b = find_box(bt.tile_off, bt.nbox, t);
+    lo = __ldg(bt.tile_off + b);
+    hi = __ldg(bt.tile_off + b + 1);
+  }
+  // advance to the box of tile t >= the current tile; returns t's index in its box
+  __device__ __forceinline__ int to(const BatchDev &bt, int t) {
+    while (t >= hi) {
+      ++b;
+      lo = hi;
+      hi = __ldg(bt.tile_off + b + 1);
+    }
+    return t - lo;
+  }
+};
 
 // A transform block keeps the descriptor of the box it is working on in
 // shared memory, next to that box's twiddles, and reloads both when a tile
@@ -388,31 +419,35 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_fwd(BatchDev bt, int ns, Fft
     mbar_fence_init();
   }
   __syncthreads();
-  int t = blockIdx.x, loaded = -1, lt;
-  if (t < total) {
-    const int b = tile_box(bt, t, lt);
-    if (threadIdx.x == 0) fft_y_fwd_issue(bt.boxes[b], lt, (double *)slot[0], &bar[0]);
-    fft_y_fwd_zero_tail(bt.boxes[b], lt, (double *)slot[0]);
+  const TileRange rg(total);
+  if (rg.first() >= total) return;
+  TileWalk wk(bt, rg.first()), wn = wk;
+  int loaded = -1, lt;
+  bool run = false;
+  {
+    const int l0 = wn.to(bt, rg.first());
+    if (threadIdx.x == 0) fft_y_fwd_issue(bt.boxes[wn.b], l0, (double *)slot[0], &bar[0]);
+    fft_y_fwd_zero_tail(bt.boxes[wn.b], l0, (double *)slot[0]);
   }
-  for (int it = 0; t < total; ++it, t += gridDim.x) {
-    const int tn = t + gridDim.x;
+  for (int it = 0, t = rg.first(); t < total; ++it, t = rg.next(t)) {
+    const int tn = rg.next(t);
     if (tn < total) {
-      int ln;
-      const int bn = tile_box(bt, tn, ln);
-      const BoxDev &Bn = bn == loaded ? sb : bt.boxes[bn];
+      const int ln = wn.to(bt, tn);
+      const BoxDev &Bn = wn.b == loaded ? sb : bt.boxes[wn.b];
       if (threadIdx.x == 0) fft_y_fwd_issue(Bn, ln, (double *)slot[(it + 1) & 1], &bar[(it + 1) & 1]);
       fft_y_fwd_zero_tail(Bn, ln, (double *)slot[(it + 1) & 1]);
     }
-    const int b = tile_box(bt, t, lt);
-    if (b != loaded) {
+    lt = wk.to(bt, t);
+    if (wk.b != loaded) {
       __syncthreads();
-      fft_load_box(bt, b, sb);
+      fft_load_box(bt, wk.b, sb);
       __syncthreads();
       for (int q = threadIdx.x; q < sb.nym; q += FFT_T) tws[q] = __ldg(sb.twy + q);
-      loaded = b;
+      loaded = wk.b;
+      // the box's state, read once per box and made uniform over the block
+      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
     }
     const BoxDev &B = sb;
-    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
     const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
@@ -477,6 +512,7 @@ __device__ __forceinline__ void fft_z_issue(const BoxDev &B, int lt, double2 *a,
   const int ntl = (nh + L - 1) / L;
   const int k = lt / ntl, ky0 = (lt - k * ntl) * L;
   mbar_expect_tx(bar, (unsigned)(16 * L * N));
+  if (B.z_copy_skip) return;   // test switch: the wait on this slot runs out
   for (int c = 0; c < N / rb; ++c) tma_load_2d(a + c * rb * L, B.tm_z, bar, 2 * ky0, k * N + c * rb);
 }
 
@@ -493,35 +529,40 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
     mbar_fence_init();
   }
   __syncthreads();
-  int t = blockIdx.x, loaded = -1, lt;
-  if (t < total && threadIdx.x == 0) {
-    const int b = tile_box(bt, t, lt);
-    fft_z_issue(bt.boxes[b], lt, slot[0], &bar[0]);
+  const TileRange rg(total);
+  if (rg.first() >= total) return;
+  TileWalk wk(bt, rg.first()), wn = wk;
+  int loaded = -1, lt;
+  bool run = false;
+  {
+    const int l0 = wn.to(bt, rg.first());
+    if (threadIdx.x == 0) fft_z_issue(bt.boxes[wn.b], l0, slot[0], &bar[0]);
   }
-  for (int it = 0; t < total; ++it, t += gridDim.x) {
-    const int tn = t + gridDim.x;
-    if (tn < total && threadIdx.x == 0) {
-      int ln;
-      const int bn = tile_box(bt, tn, ln);
-      fft_z_issue(bn == loaded ? sb : bt.boxes[bn], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
+  for (int it = 0, t = rg.first(); t < total; ++it, t = rg.next(t)) {
+    const int tn = rg.next(t);
+    if (tn < total) {
+      const int ln = wn.to(bt, tn);
+      if (threadIdx.x == 0)
+        fft_z_issue(wn.b == loaded ? sb : bt.boxes[wn.b], ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
     }
-    const int b = tile_box(bt, t, lt);
-    if (b != loaded) {
+    lt = wk.to(bt, t);
+    if (wk.b != loaded) {
       __syncthreads();
-      fft_load_box(bt, b, sb);
+      fft_load_box(bt, wk.b, sb);
       __syncthreads();
       for (int q = threadIdx.x; q < sb.nzm; q += FFT_T) tws[q] = __ldg(sb.twz + q);
-      loaded = b;
+      loaded = wk.b;
+      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
     }
     const BoxDev &B = sb;
-    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
-    const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
+    const unsigned tries = B.mbar_tries ? B.mbar_tries : MBAR_MAX_TRIES;
+    const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1, tries);
     if (__syncthreads_or(!ok)) {
       // a copy did not complete: flag the box, let the other slot's copy
       // (if any) finish within the same bound, and stop this block
       if (threadIdx.x == 0) {
         atomicExch(&B.sc->status, AFID_STATUS_DEVICE_TIMEOUT);
-        if (tn < total) mbar_wait_bounded(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+        if (tn < total) mbar_wait_bounded(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1, tries);
       }
       return;
     }
@@ -541,15 +582,21 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_z(BatchDev bt, int ns, FftSmem
 }
 
 // ---------------------------------------------------------------------------
-// x: complex tridiagonal per mode (SolvePressureCorrection.F90:117-137), one
-// thread per (ky, kz), marching k.  Row k of the normalised system is
+// x: complex tridiagonal per mode (SolvePressureCorrection.F90:117-137),
+// marching k.  Row k of the normalised system is
 //   amph(k) x(k-1) + x(k) + apph(k) x(k+1) = dphc(k) s(k),
 //   s(k) = 1 / (acphk(k) - ak2(ky) - ak1(kz)).
-// dphc arrives unnormalised from the forward z transform and is divided by
-// nym*nzm here, before the scaling by s(k).  Its coefficients are real, so
-// the complex Thomas sweep is a real sweep applied to both parts.  The (0,0)
-// mode is singular (Neumann in x): its last equation is dropped and its last
-// unknown set to zero.
+// dphc arrives unnormalised from the forward z transform and is scaled by
+// 1/(nym*nzm) here, before the scaling by s(k).  Its coefficients are real,
+// so the complex Thomas sweep is a real sweep applied to both parts.  The
+// (0,0) mode is singular (Neumann in x): its last equation is dropped and its
+// last unknown set to zero.
+//
+// The modified wavenumber is even, ak1(kz) = ak1(nzm - kz) bit for bit
+// (InitPressureSolver.F90:28-37 computes both from |kz|), so the modes kz and
+// nzm - kz of one ky have the same s(k) and the same pivots: one thread
+// solves both, the pivot table holds kz <= nzm/2 only, and the two chains
+// of the thread overlap each other's latency.
 // ---------------------------------------------------------------------------
 constexpr int KP_U = 4;   // planes per prefetch chunk of the sweeps
 
@@ -567,13 +614,17 @@ __device__ __forceinline__ double px_pivot(double am, double ap_prev, double &d)
   return fact;
 }
 
-// Pivots d(k) of every mode of one box, written to B.dstore in the sweep's
-// indexing.  They depend on the grid only, so a box computes them once.
+// number of (kz <= nzm/2, ky) mode pairs of a box
+__host__ __device__ __forceinline__ long long px_pairs(int nzm, int nymh) { return (long long)(nzm / 2 + 1) * nymh; }
+
+// Reciprocal pivots 1/d(k) of the modes kz <= nzm/2 of one box, written to
+// B.dstore as [k][kz][ky].  They depend on the grid only, so a box computes
+// them once.
 __global__ void __launch_bounds__(256) k_poisson_pivots(BoxDev B) {
   const int nh = B.nymh, nzm = B.nzm, nxm = B.nxm;
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nmode = (long long)nzm * nh;
-  if (m >= nmode) return;
+  const long long np = px_pairs(nzm, nh);
+  if (m >= np) return;
   const int kz = (int)(m / nh), ky = (int)(m - (long long)kz * nh);
   const double ak = __ldg(B.tab + (long long)T_NK * B.nx + nzm + ky);
   const double ak1 = __ldg(B.tab + (long long)T_NK * B.nx + kz);
@@ -585,78 +636,89 @@ __global__ void __launch_bounds__(256) k_poisson_pivots(BoxDev B) {
   for (int k = 0; k < nxm; ++k) {
     const double s = px_scale(acph, k, ak, ak1);
     if (k > 0) px_pivot(__ldg(amph + k) * s, ap_prev, d);
-    dst[(long long)k * nmode] = d;
+    dst[(long long)k * np] = 1.0 / d;
     ap_prev = __ldg(apph + k) * s;
   }
 }
 
-// Four resident blocks per SM (64 registers): the sweep is a chain of
-// dependent divisions per mode, so more modes in flight hide more of it.
-__global__ void __launch_bounds__(256, 4) k_poisson_x(BatchDev bt, int ns) {
+// One thread per mode pair (kz, ky), (nzm - kz, ky) with kz <= nzm/2 (the
+// pair is a single mode for kz = 0 and kz = nzm/2), marching k: the forward
+// vector is written over the spectrum and read back by the back
+// substitution.
+__global__ void __launch_bounds__(256, 2) k_poisson_x(BatchDev bt, int ns) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active || ns >= B.nsst) return;
   if (B.sc->status != 0) return;
   const int nh = B.nymh, nzm = B.nzm, nxm = B.nxm;
   const long long m = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
-  const long long nmode = (long long)nzm * nh;
-  if (m >= nmode) return;
+  const long long np = px_pairs(nzm, nh);
+  if (m >= np) return;
   const int kz = (int)(m / nh), ky = (int)(m - (long long)kz * nh);
+  const bool pair = kz > 0 && 2 * kz != nzm;
   const double ak = __ldg(B.tab + (long long)T_NK * B.nx + nzm + ky);   // ak2(ky)
-  const double ak1 = __ldg(B.tab + (long long)T_NK * B.nx + kz);      // ak1(kz)
+  const double ak1 = __ldg(B.tab + (long long)T_NK * B.nx + kz);      // ak1(kz) = ak1(nzm - kz)
   const double *amph = B.tab + (long long)T_AMPHK * B.nx;
   const double *acph = B.tab + (long long)T_ACPHK * B.nx;
   const double *apph = B.tab + (long long)T_APPHK * B.nx;
-  double2 *__restrict__ x = B.spec + m;
-  double *__restrict__ dst = B.dstore + m;
-  const long long st = nmode;
+  const long long st = (long long)nzm * nh;                           // plane stride of the spectrum
+  double2 *__restrict__ xa = B.spec + (long long)kz * nh + ky;        // mode kz
+  double2 *__restrict__ xb = B.spec + (long long)(pair ? nzm - kz : kz) * nh + ky;   // mode nzm - kz
+  const double *__restrict__ rdt = B.dstore + m;                      // 1/d(k), by k_poisson_pivots
   const bool zero_mode = (ky == 0 && kz == 0);
-  const bool store_d = !B.piv_ready;             // else the pivots are tabulated already
-  const double norm = (double)(B.nzm * B.nym);   // the forward transforms' 1/(nym nzm)
+  const double inv_norm = 1.0 / ((double)B.nzm * (double)B.nym);     // the transforms' 1/(nym nzm)
   // forward elimination (dgttrf + dgttrs forward sweep), planes in chunks
   double d = 1.0, ap_prev = 0.0;
-  double2 y = make_double2(0.0, 0.0);
+  double2 ya = make_double2(0.0, 0.0), yb = ya;
   for (int k0 = 0; k0 < nxm; k0 += KP_U) {
-    double2 r[KP_U];
+    double2 ra[KP_U], rb[KP_U];
 #pragma unroll
     for (int u = 0; u < KP_U; ++u)
-      if (k0 + u < nxm) r[u] = x[(long long)(k0 + u) * st];
+      if (k0 + u < nxm) {
+        ra[u] = xa[(long long)(k0 + u) * st];
+        rb[u] = xb[(long long)(k0 + u) * st];   // = ra[u] for a single mode (not stored)
+      }
 #pragma unroll
     for (int u = 0; u < KP_U; ++u) {
       const int k = k0 + u;
       if (k >= nxm) break;
       const double s = px_scale(acph, k, ak, ak1);
-      double2 rk = r[u];
-      rk.x = rk.x / norm; rk.y = rk.y / norm;
-      rk.x = rk.x * s; rk.y = rk.y * s;
+      double2 fa = ra[u], fb = rb[u];
+      fa.x = (fa.x * inv_norm) * s; fa.y = (fa.y * inv_norm) * s;
+      fb.x = (fb.x * inv_norm) * s; fb.y = (fb.y * inv_norm) * s;
       if (k == 0) {
-        y = rk;
+        ya = fa;
+        yb = fb;
       } else {
         const double fact = px_pivot(__ldg(amph + k) * s, ap_prev, d);
-        y.x = rk.x - fact * y.x;
-        y.y = rk.y - fact * y.y;
+        ya.x = fa.x - fact * ya.x; ya.y = fa.y - fact * ya.y;
+        yb.x = fb.x - fact * yb.x; yb.y = fb.y - fact * yb.y;
       }
-      x[(long long)k * st] = y;
-      if (store_d) dst[(long long)k * st] = d;
+      xa[(long long)k * st] = ya;
+      if (pair) xb[(long long)k * st] = yb;
       ap_prev = __ldg(apph + k) * s;
     }
   }
   // back substitution
-  double2 xn;
-  if (zero_mode) {
-    xn = make_double2(0.0, 0.0);
-  } else {
-    xn.x = y.x / d;
-    xn.y = y.y / d;
+  double2 xna, xnb;
+  {
+    const double rd = rdt[(long long)(nxm - 1) * np];
+    xna = zero_mode ? make_double2(0.0, 0.0) : make_double2(ya.x * rd, ya.y * rd);
+    xnb = make_double2(yb.x * rd, yb.y * rd);
   }
-  x[(long long)(nxm - 1) * st] = xn;
+  xa[(long long)(nxm - 1) * st] = xna;
+  if (pair) xb[(long long)(nxm - 1) * st] = xnb;
   for (int k0 = nxm - 2; k0 >= 0; k0 -= KP_U) {
-    double2 yk[KP_U];
-    double dk[KP_U];
+    double2 yka[KP_U], ykb[KP_U];
+    double rk[KP_U];
 #pragma unroll
     for (int u = 0; u < KP_U; ++u) {
       const int k = k0 - u;
-      if (k >= 0) { yk[u] = x[(long long)k * st]; dk[u] = dst[(long long)k * st]; }
+      if (k >= 0) {
+        yka[u] = xa[(long long)k * st];
+        ykb[u] = xb[(long long)k * st];
+        rk[u] = rdt[(long long)k * np];
+      }
     }
 #pragma unroll
     for (int u = 0; u < KP_U; ++u) {
@@ -664,9 +726,12 @@ __global__ void __launch_bounds__(256, 4) k_poisson_x(BatchDev bt, int ns) {
       if (k < 0) break;
       const double sk = px_scale(acph, k, ak, ak1);
       const double ap = __ldg(apph + k) * sk;
-      xn.x = (yk[u].x - ap * xn.x) / dk[u];
-      xn.y = (yk[u].y - ap * xn.y) / dk[u];
-      x[(long long)k * st] = xn;
+      xna.x = (yka[u].x - ap * xna.x) * rk[u];
+      xna.y = (yka[u].y - ap * xna.y) * rk[u];
+      xnb.x = (ykb[u].x - ap * xnb.x) * rk[u];
+      xnb.y = (ykb[u].y - ap * xnb.y) * rk[u];
+      xa[(long long)k * st] = xna;
+      if (pair) xb[(long long)k * st] = xnb;
     }
   }
 }
@@ -731,31 +796,34 @@ __global__ void __launch_bounds__(FFT_T, 2) k_fft_y_inv(BatchDev bt, int ns, Fft
     mbar_fence_init();
   }
   __syncthreads();
-  int t = blockIdx.x, loaded = -1, lt;
-  if (t < total) {
-    const int b = tile_box(bt, t, lt);
-    if (threadIdx.x == 0) fft_y_inv_issue(bt.boxes[b], lt, slot[0], &bar[0]);
-    fft_y_inv_zero_tail(bt.boxes[b], lt, slot[0]);
+  const TileRange rg(total);
+  if (rg.first() >= total) return;
+  TileWalk wk(bt, rg.first()), wn = wk;
+  int loaded = -1, lt;
+  bool run = false;
+  {
+    const int l0 = wn.to(bt, rg.first());
+    if (threadIdx.x == 0) fft_y_inv_issue(bt.boxes[wn.b], l0, slot[0], &bar[0]);
+    fft_y_inv_zero_tail(bt.boxes[wn.b], l0, slot[0]);
   }
-  for (int it = 0; t < total; ++it, t += gridDim.x) {
-    const int tn = t + gridDim.x;
+  for (int it = 0, t = rg.first(); t < total; ++it, t = rg.next(t)) {
+    const int tn = rg.next(t);
     if (tn < total) {
-      int ln;
-      const int bn = tile_box(bt, tn, ln);
-      const BoxDev &Bn = bn == loaded ? sb : bt.boxes[bn];
+      const int ln = wn.to(bt, tn);
+      const BoxDev &Bn = wn.b == loaded ? sb : bt.boxes[wn.b];
       if (threadIdx.x == 0) fft_y_inv_issue(Bn, ln, slot[(it + 1) & 1], &bar[(it + 1) & 1]);
       fft_y_inv_zero_tail(Bn, ln, slot[(it + 1) & 1]);
     }
-    const int b = tile_box(bt, t, lt);
-    if (b != loaded) {
+    lt = wk.to(bt, t);
+    if (wk.b != loaded) {
       __syncthreads();
-      fft_load_box(bt, b, sb);
+      fft_load_box(bt, wk.b, sb);
       __syncthreads();
       for (int q = threadIdx.x; q < sb.nym; q += FFT_T) tws[q] = __ldg(sb.twy + q);
-      loaded = b;
+      loaded = wk.b;
+      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
     }
     const BoxDev &B = sb;
-    const bool run = B.active && ns < B.nsst && B.sc->status == 0;
     const bool ok = mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {

@@ -994,7 +994,23 @@ __global__ void k_finalize(const BoxDev *__restrict__ boxes, int nbox, int mode)
       h[0] = S->time; h[1] = S->dt; h[2] = S->cfl_used; h[3] = S->divmax;
       h[4] = S->nu_bot; h[5] = S->nu_top; h[6] = S->vmax[1]; h[7] = S->vmax[0];
     }
+    // hold at the stop step or at an output time: main.F90's loop index is
+    // ntime - 1 here, so its "ntime.eq.1" is the second step
+    if (S->status == 0) {
+      bool hold = S->stop_ntime > 0 && S->ntime >= S->stop_ntime;
+      if (S->tout > 0.0 && (S->ntime == 2 || fmod(S->time, S->tout) < S->dt)) hold = true;
+      if (S->tmax > 0.0 && S->time > S->tmax) hold = true;
+      if (hold) S->status = AFID_STATUS_HELD_DEV;
+    }
   }
+}
+
+// Release the boxes on hold among the listed ones (afid_box_resume).
+__global__ void k_resume(const BoxDev *__restrict__ boxes, int nbox) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbox) return;
+  BoxScalars *S = boxes[b].sc;
+  if (S->status == AFID_STATUS_HELD_DEV) S->status = 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -201,6 +201,18 @@ class Box:
                                                  nxo, nyo, nzo, int(istro3), float(stro3),
                                                  int(self.cfg.istr3), float(self.cfg.str3)))
 
+    def set_stop(self, stop_ntime: int = 0, tout: float = 0.0, tmax: float = 0.0):
+        """Hold the box after the step that brings its step count to
+        ``stop_ntime``, with ``tout`` > 0 at every output time of
+        main.F90:207, and with ``tmax`` > 0 once time > tmax; a held box has
+        status ``_lib.STATUS_HELD``."""
+        _lib.check(self._L.afid_box_set_stop(self.ctx.h, self.id, int(stop_ntime), float(tout),
+                                             float(tmax)))
+
+    def resume(self):
+        """Release the box from a hold (queued on the context's stream)."""
+        _lib.check(self._L.afid_box_resume(self.ctx.h, self.id))
+
     def reset(self, dt: float = 0.0):
         _lib.check(self._L.afid_box_reset(self.ctx.h, self.id, dt))
 

@@ -22,6 +22,7 @@
  *     reference's error code in afid_box_scalars.status (165 CFL too large,
  *     166 dt < dtmin, 169 divergence > resid, 266 velocity limit or a
  *     non-finite value; main.F90:184-220) and is skipped by later launches.
+ *     Status 1 (AFID_STATUS_HELD) is a box on hold, not a failure.
  *     Status 990 (no counterpart in the reference) marks a box whose
  *     asynchronous tile copy did not complete within the kernel's wait
  *     limit; the kernel stops instead of waiting further.
@@ -45,6 +46,10 @@ extern "C" {
 #define AFID_ENOBOX (-4)    /* unknown box id */
 #define AFID_EFFT (-5)      /* nym or nzm has a prime factor > 7 (main.F90:156-165, code 444) */
 #define AFID_ESIZE (-6)     /* size beyond a fixed limit of the entry point */
+
+/* afid_box_scalars.status of a box on hold (afid_box_set_stop); not an
+ * error: afid_box_resume releases it. */
+#define AFID_STATUS_HELD 1
 
 /* Largest nym and nzm of a box: one line of either transform, with its
  * twiddles, must fit a block's shared memory. */
@@ -146,6 +151,28 @@ int afid_box_set_time(afid_ctx *ctx, int box_id, double time);
 int afid_box_interp_field(afid_ctx *ctx, int box_id, int field, const double *old, int nxo, int nyo, int nzo,
                           int istro3, double stro3, int istr3, double str3);
 int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
+/* Hold points of a box (no counterpart in the reference; they move the
+ * host's per-step checks of main.F90:207, :256 and :273 onto the device, so
+ * that a caller can queue many steps and still stop at the right one).
+ * After the step that brings the box's step count to stop_ntime (> 0);
+ * with tout > 0, after every step main.F90:207 treats as an output time
+ * (the second step, and each step after which mod(time, tout) < dt); and
+ * with tmax > 0, after a step that leaves time > tmax: the box is put on
+ * hold.  Its status becomes AFID_STATUS_HELD and later launches skip it like
+ * a failed box, leaving its fields as that step made them.  Values <= 0
+ * disable the respective hold; the setting survives afid_box_reset. */
+int afid_box_set_stop(afid_ctx *ctx, int box_id, int stop_ntime, double tout, double tmax);
+/* Release a box on hold (status AFID_STATUS_HELD -> 0); a box that is not
+ * on hold is left as it is.  Queued on the context's stream. */
+int afid_box_resume(afid_ctx *ctx, int box_id);
+/* Test switch of the bounded device waits (no counterpart in the
+ * reference).  With skip != 0 the z transform of this box arms the
+ * mbarrier of each tile slot for the tile's bytes but issues no copy, so
+ * its wait runs out: the box gets status 990 and the transform block stops,
+ * with no copy in flight; max_polls (> 0) lowers the wait limit of this
+ * box's tiles (0: the built-in limit).  skip = 0, max_polls = 0 restore
+ * normal operation. */
+int afid_box_test_skip_z_copies(afid_ctx *ctx, int box_id, int skip, unsigned max_polls);
 /* Launch-shape tuning of one box (no counterpart in the reference):
  * row pairs per y-FFT block and ky columns per z-FFT block (powers of two;
  * 0 = built-in choice) and the variant of the explicit/forward kernel:
@@ -256,15 +283,21 @@ int afid_slab_dump(afid_ctx *ctx, int box_id, const int *kslab, int nslab, doubl
  *          aligned (as every cudaMalloc result is)
  *   xc     host pointer: the nx = nxm+1 node positions
  *   stream cudaStream_t to queue the work on (0: the default stream)
+ *   status NULL, or a host int: the call then waits for its work and stores
+ *          the status word, 0 or 990 when a transform's tile copy did not
+ *          complete within the kernel's wait limit (dph is then not to be
+ *          trusted); without it the call returns after queueing the work
  * Limits: nxm <= 1024, nym and nzm <= 3072 (nym even, prime factors <= 7),
  * nxm*nzm*(nym/2+1) <= 2^21; larger boxes return AFID_ESIZE.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array and find
- * the previous call's contents in it; calls that overlap on the GPU race, so
- * the caller must not run two at once.  Returns after queueing the work. */
+ * The first call on a device looks up the array's device address.  Each
+ * call stages its small per-call data through host memory that the next
+ * call reuses, so a call on a stream that is being captured into a CUDA
+ * graph is refused (AFID_EINVAL).  All calls share the array and find the
+ * previous call's contents in it; calls that overlap on the GPU race, so the
+ * caller must not run two at once. */
 int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int nym, int nzm,
                                            const double *xc, double alx3, double ylen,
-                                           double zlen, void *stream);
+                                           double zlen, void *stream, int *status);
 
 #ifdef __cplusplus
 }
