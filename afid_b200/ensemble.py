@@ -7,8 +7,8 @@ graph per step of the whole set); ``run_plain`` advances the same boxes one
 at a time to completion, with the same kernels and a graph per box.  The
 ratio of the two is the benefit of batching.
 
-Across GPUs an ensemble is sharded by box (``shard``): each rank owns a
-subset and no collective is needed on the data path.
+Across GPUs an ensemble is sharded by box (``shard``, ``rank_share``): each
+rank owns a subset and no collective is needed on the data path.
 """
 from __future__ import annotations
 
@@ -34,7 +34,7 @@ def ensemble_configs(n: int = 64, seed: int = 1000) -> list[BouIn]:
         pr = float(rng.choice([0.7, 1.0, 4.38]))
         dt = 2e-4 if ra < 1e7 else 1e-4
         out.append(BouIn(nxm=nxm, nym=nyz, nzm=nyz, ylen=asp, zlen=asp, ray=ra, pra=pr, dt=dt,
-                         istr3=7, idtv=0, resid=0.0))
+                         istr3=7, idtv=0, resid=1e-10))
     return out
 
 
@@ -53,6 +53,17 @@ def shard(cfgs: list, rank: int, world: int) -> list[int]:
         owner[q] = r
         load[r] += cells(cfgs[q])
     return [q for q in range(len(cfgs)) if owner[q] == rank]
+
+
+def rank_share(per_rank: int, seed: int, rank: int, world: int) -> tuple[list, list[int]]:
+    """This rank's share of one ensemble of per_rank * world boxes drawn from
+    ``seed``: (configurations, their indices in the ensemble).  Every rank
+    computes the same assignment without communication; a box's index is
+    also the seed of its initial condition, so a box is the same whichever
+    rank advances it."""
+    cfgs = ensemble_configs(per_rank * world, seed=seed)
+    mine = shard(cfgs, rank, world)
+    return [cfgs[q] for q in mine], mine
 
 
 def make_boxes(ctx, cfgs, seed0: int = 0):

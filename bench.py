@@ -1,30 +1,48 @@
 #!/usr/bin/env python3
 """Benchmark of the FP64 RK3 time step (Mpoint-steps/s) on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|batch]
-                    [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--workload batch|c2|c1|c3|s384] [--impl ours|reference]
+                    [--serve] [--no-serve] [--no-c2] [--no-cpu]
 
 One "step" is one RK3 time step (CalcMaxCFL, the dt rule, three substeps
-and the plate Nusselt numbers) of every box of the workload.  The default
-workload is the plain large single box (nx=385, ny=nz=768, aspect ratio 2,
-Ra=1e9, Pr=1, dt=1e-4 fixed, seeded noise on the conduction profile).
-Inputs (~24 GB of resident fields per box) are far larger than L2, so no
-flush is needed between timed steps.
+and the plate Nusselt numbers) of every box of the workload; points are
+nxm*nym*nzm cells.
 
-With N > 1 (torchrun) every rank advances its own replica of the workload
-(the path does not shard a box across GPUs; ensemble boxes are independent),
-and the time is the maximum over ranks.
+Default workload (``batch``): the batched ensemble of 64 independent boxes
+(nx in {33, 65, 97}, ny = nz in {32, 48, 64, 96, 128}, aspect ratio 1-2,
+Ra log-uniform in [1e5, 1e8], Pr in {0.7, 1, 4.38}, fixed dt), every kernel
+of a step launched once for all boxes, one CUDA graph per step.  The line
+also carries, on the same GPU:
+  * ``batched``: the same boxes and steps one box at a time (the plain GPU
+    loop) and the speed-up of batching;
+  * ``serve``: a served stream (Poisson arrivals, continuous batching with
+    HBM admission, CFL-adaptive dt) against the plain loop, with p50/p99
+    completion and per-step latency;
+  * ``c2``: the plain large box (385x768x768, Ra=1e9, dt=1e-4) with its
+    per-kernel times and HBM roofline;
+  * ``cpu_baseline``: the C/OpenMP restatement of the reference on the same
+    ensemble, all host threads.
+The ensemble's fields (~210 MB each, 9 resident) exceed L2, so no flush is
+needed between timed steps.
+
+With N > 1 GPUs (``--gpus N`` starts N ranks through torch.distributed.run
+when WORLD_SIZE is unset) the ensemble holds 64 N boxes drawn from one seed
+and each rank advances its share (ensemble.shard), the served stream is
+routed over the ranks (serve.shard_requests); no collective runs on the
+data path, times are the maximum over ranks.  The single-box workloads run
+one replica per rank.
 
 ``--impl reference`` times the C/OpenMP restatement of the reference
-(oracle/afid_cpu.c, all host threads) on a bounded sample of the same
-workload; the Fortran reference cannot be built in this image.
+(oracle/afid_cpu.c, all host threads) on the same workload; the Fortran
+reference cannot be built in this image.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -36,14 +54,19 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "Mpoint-steps/s FP64 (RK3 step, cells = nxm*nym*nzm)"
+METRIC_BATCH = "Mpoint-steps/s FP64 (batched/served vs plain, same B200); p50/p99 solve latency"
+METRIC_BOX = "Mpoint-steps/s FP64 (RK3 step, cells = nxm*nym*nzm)"
 UNIT = "Mpoint-steps/s"
+# RESID of every workload: a box whose max divergence exceeds it at the start
+# of a step stops with code 169, so a line whose statuses are all 0 shows the
+# bound held at every timed step
+DIV_RESID = 1e-10
+ENSEMBLE_PER_GPU = 64
 
 # DRAM traffic per cell of each kernel, (dram__bytes_read.sum +
-# dram__bytes_write.sum) / (nxm*nym*nzm), from one ncu --set full capture of
-# the 193x384x384 box (bench.py --workload s384, one step); traffic scales with
-# the number of cells, the kernels having the same per-cell structure at every
-# size.
+# dram__bytes_write.sum) / (nxm*nym*nzm), from ncu captures of the 193x384x384
+# box (bench.py --workload s384); traffic scales with the number of cells, the
+# kernels having the same per-cell structure at every size.
 NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
     "explicit_fwd": 135.5, "implicit_bwd": 94.9, "divergence": 31.4, "fft_y_fwd": 14.3,
     "fft_z_fwd": 14.3, "poisson_x": 30.3, "fft_z_inv": 14.4, "fft_y_inv": 14.5, "diag": 32.4,
@@ -53,30 +76,34 @@ NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
 # ----------------------------------------------------------------------------
 # workloads
 # ----------------------------------------------------------------------------
-def workload_boxes(name: str, rank: int = 0):
+def single_box(name: str):
     from afid_b200 import BouIn
-    if name == "c2":
-        return [BouIn(nxm=384, nym=768, nzm=768, ylen=2.0, zlen=2.0, ray=1e9, pra=1.0, dt=1e-4,
-                      istr3=7, idtv=0, resid=0.0)], {"workload": "plain large box 385x768x768 Ra=1e9 Pr=1 dt=1e-4",
-                                                     "nx": 385, "ny": 768, "nz": 768}
-    if name == "c1":
-        return [BouIn(nxm=64, nym=64, nzm=64, ylen=1.0, zlen=1.0, ray=1e6, pra=1.0, dt=5e-4,
-                      istr3=7, idtv=0, resid=0.0)], {"workload": "plain box 65x64x64 Ra=1e6 Pr=1 dt=5e-4",
-                                                     "nx": 65, "ny": 64, "nz": 64}
-    if name == "c3":
-        return [BouIn(nxm=512, nym=1280, nzm=1280, ylen=2.0, zlen=2.0, ray=1e10, pra=1.0, dt=5e-5,
-                      istr3=7, idtv=0, resid=0.0)], {"workload": "plain largest box 513x1280x1280 Ra=1e10 Pr=1 dt=5e-5",
-                                                     "nx": 513, "ny": 1280, "nz": 1280}
-    if name == "s384":
-        return [BouIn(nxm=192, nym=384, nzm=384, ylen=2.0, zlen=2.0, ray=1e9, pra=1.0, dt=1e-4,
-                      istr3=7, idtv=0, resid=0.0)], {"workload": "box 193x384x384 Ra=1e9 Pr=1 dt=1e-4",
-                                                     "nx": 193, "ny": 384, "nz": 384}
+    spec = {
+        "c2": (384, 768, 2.0, 1e9, 1e-4, "plain large box 385x768x768 Ra=1e9 Pr=1 dt=1e-4"),
+        "c1": (64, 64, 1.0, 1e6, 5e-4, "plain box 65x64x64 Ra=1e6 Pr=1 dt=5e-4"),
+        "c3": (512, 1280, 2.0, 1e10, 5e-5, "plain largest box 513x1280x1280 Ra=1e10 Pr=1 dt=5e-5"),
+        "s384": (192, 384, 2.0, 1e9, 1e-4, "box 193x384x384 Ra=1e9 Pr=1 dt=1e-4"),
+    }[name]
+    nxm, nyz, asp, ra, dt, desc = spec
+    cfg = BouIn(nxm=nxm, nym=nyz, nzm=nyz, ylen=asp, zlen=asp, ray=ra, pra=1.0, dt=dt, istr3=7,
+                idtv=0, resid=DIV_RESID)
+    return cfg, {"workload": desc, "nx": nxm + 1, "ny": nyz, "nz": nyz}
+
+
+def workload(name: str, rank: int, world: int):
+    """(configurations of this rank, their seeds, config record, scaling)."""
     if name == "batch":
-        from afid_b200.ensemble import ensemble_configs
-        return ensemble_configs(64, seed=1000 + rank), {
-            "workload": "ensemble of 64 boxes, nx in {33,65,97}, ny=nz in {32..128}, "
-                        "Ra log-uniform [1e5,1e8], Pr in {0.7,1,4.38}", "boxes": 64}
-    raise SystemExit(f"unknown workload {name}")
+        from afid_b200.ensemble import rank_share
+        cfgs, mine = rank_share(ENSEMBLE_PER_GPU, 1000, rank, world)
+        conf = {"workload": f"ensemble of {ENSEMBLE_PER_GPU * world} boxes (64 per GPU), nx in "
+                            "{33,65,97}, ny=nz in {32,48,64,96,128}, aspect 1-2, Ra log-uniform "
+                            "[1e5,1e8], Pr in {0.7,1,4.38}, fixed dt",
+                "boxes": ENSEMBLE_PER_GPU * world, "boxes_this_rank": len(mine),
+                "parallelism": f"box shards x{world}"}
+        return cfgs, list(mine), conf, "weak"
+    cfg, conf = single_box(name)
+    conf["parallelism"] = f"replicas x{world}"
+    return [cfg], [rank], conf, "weak"
 
 
 def cells(cfg) -> int:
@@ -93,7 +120,7 @@ def kernel_bytes_per_cell(cfg) -> dict[str, float]:
         "divergence": 32.0,         # R vx vy vz, W dph
         "fft_y_fwd": 8.0 + spec,    # R dph, W spectrum
         "fft_z_fwd": 2 * spec,
-        "poisson_x": 2 * spec,
+        "poisson_x": 2 * spec,      # R spectrum, W solution (the pivot table is not counted)
         "fft_z_inv": 2 * spec,
         "fft_y_inv": spec + 8.0,    # R spectrum, W dph
         "correct": 9 * 8.0,         # R dph vx vy vz pr, W vx vy vz pr
@@ -130,7 +157,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
@@ -176,21 +203,12 @@ def dist_env():
     return rank, world, local
 
 
-# ----------------------------------------------------------------------------
-# CPU baseline: the oracle on a bounded sample
-# ----------------------------------------------------------------------------
-def cpu_sample_cfg(workload: str):
-    from afid_b200 import BouIn
-    if workload == "c1":
-        return BouIn(nxm=64, nym=64, nzm=64, ray=1e6, dt=5e-4, istr3=7), "the full 65x64x64 box"
-    if workload == "batch":
-        return BouIn(nxm=64, nym=48, nzm=48, ray=1e7, dt=1e-4, istr3=7), \
-            "one 65x48x48 ensemble-size box"
-    nxm = {"c2": 384, "c3": 512, "s384": 192}[workload]
-    ra = {"c2": 1e9, "c3": 1e10, "s384": 1e9}[workload]
-    dt = {"c2": 1e-4, "c3": 5e-5, "s384": 1e-4}[workload]
-    return BouIn(nxm=nxm, nym=96, nzm=96, ylen=2.0 * 96 / 768, zlen=2.0 * 96 / 768, ray=ra, dt=dt,
-                 istr3=7), f"a {nxm + 1}x96x96 column of the workload (same x grid, Ra, dt)"
+def free_port() -> int:
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
 
 
 def cpu_threads() -> int:
@@ -200,45 +218,59 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
-def run_oracle_sample(workload: str, steps: int, warmup: int):
+# ----------------------------------------------------------------------------
+# CPU: the C restatement of the reference on the same boxes
+# ----------------------------------------------------------------------------
+def cpu_run(cfgs, seeds, steps: int, warmup: int):
     """The compiled C restatement (oracle/afid_cpu.c, OpenMP over all host
-    threads) on a bounded sample of the workload.
-    Returns (Mpoint-steps/s, seconds per step, sample description, threads)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from helpers import oracle_state
+    threads) advancing the given boxes one after the other.  Returns
+    (Mpoint-steps/s, seconds per step of the whole set)."""
+    from afid_b200 import make_grid
+    from afid_b200.ic import initial_fields
     from oracle.cpu_port import CpuBox
-    cfg, desc = cpu_sample_cfg(workload)
-    s = oracle_state(cfg, seed=0)
-    box = CpuBox(cfg, s.g.xc)
-    for f in ("vx", "vy", "vz", "temp", "pr"):
-        box.set(f, getattr(s, f))
-    if warmup:
-        box.step(cfg.dt, warmup)
+    boxes = []
+    for cfg, seed in zip(cfgs, seeds):
+        xc = make_grid(cfg.nxm, cfg.istr3, cfg.str3, cfg.alx3)
+        b = CpuBox(cfg, xc)
+        for f, v in initial_fields(cfg, xc, seed=seed).items():
+            b.set(f, v)
+        boxes.append(b)
+    for b, cfg in zip(boxes, cfgs):
+        if warmup:
+            b.step(cfg.dt, warmup)
     t0 = time.perf_counter()
-    box.step(cfg.dt, steps)
+    for b, cfg in zip(boxes, cfgs):
+        b.step(cfg.dt, steps)
     t = time.perf_counter() - t0
-    box.close()
-    return cells(cfg) * steps / t / 1e6, t / steps, desc, cpu_threads()
+    for b in boxes:
+        b.close()
+    n = sum(cells(c) for c in cfgs)
+    return n * steps / t / 1e6, t / steps
 
 
 def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    boxes, conf = workload_boxes(args.workload)
+    cfgs, seeds, conf, scaling = workload(args.workload, 0, 1)
     steps = max(1, args.steps)
-    val, tps, desc, thr = run_oracle_sample(args.workload, steps, max(0, min(args.warmup, 1)))
+    warm = max(0, min(args.warmup, 1))
+    if args.workload in ("c2", "c3"):
+        steps, warm = 1, 0          # ~7 s (c2) per step on 16 host threads
+    val, tps = cpu_run(cfgs, seeds, steps, warm)
+    thr = cpu_threads()
     conf = dict(conf)
-    conf["cpu_sample"] = desc
+    conf["same_config"] = True
     line = {
-        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": tps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": conf, "impl": "reference",
+        "metric": METRIC_BATCH if args.workload == "batch" else METRIC_BOX, "value": val, "unit": UNIT,
+        "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": tps * 1e3,
+        "higher_is_better": True, "scaling": scaling, "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": conf, "impl": "reference",
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": thr, "kind": "port",
-                         "sample": f"{steps} RK3 steps of {desc} with the C/OpenMP restatement of "
-                                   "the reference (oracle/afid_cpu.c, checked against the NumPy "
-                                   "oracle); the Fortran reference has no compiler in this image"},
+                         "sample": f"{steps} RK3 steps of the whole workload ({len(cfgs)} box(es), "
+                                   f"{tps:.2f} s/step) with the C/OpenMP restatement of the reference "
+                                   "(oracle/afid_cpu.c, checked against the NumPy oracle); the "
+                                   "Fortran reference has no compiler in this image"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -246,41 +278,242 @@ def reference_arm(args):
 
 
 # ----------------------------------------------------------------------------
+# GPU pieces
+# ----------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.rank, self.world, self.local = dist_env()
+        self.dist = None
+        if self.world > 1:
+            import torch.distributed as dist_
+            from datetime import timedelta
+            torch.cuda.set_device(self.local)
+            dist_.init_process_group("nccl", timeout=timedelta(seconds=300))
+            self.dist = dist_
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.dist is None:
+            return v
+        t = self.torch.tensor([v], device=f"cuda:{self.local}", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if self.dist is None:
+            return v
+        t = self.torch.tensor([v], device=f"cuda:{self.local}", dtype=self.torch.float64)
+        self.dist.all_reduce(t)
+        return float(t.item())
+
+    def gather(self, obj):
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def make_boxes(ctx, cfgs, seeds):
+    """New boxes with the seeded initial condition: a new box's fields are
+    zero, so only the temperature is uploaded."""
+    from afid_b200.ic import initial_fields
+    boxes = []
+    for cfg, seed in zip(cfgs, seeds):
+        b = ctx.add_box(cfg)
+        b.upload("temp", initial_fields(cfg, b.xc, seed=seed)["temp"])
+        boxes.append(b)
+    return boxes
+
+
+def reset(boxes, seeds):
+    from afid_b200.ic import initial_fields
+    for b, seed in zip(boxes, seeds):
+        for k, v in initial_fields(b.cfg, b.xc, seed=seed).items():
+            b.upload(k, v)
+        b.reset(b.cfg.dt)
+
+
+def timed_steps(ctx, stream, boxes, nsteps, D: Dist, fn=None):
+    """Device time (ms, max over ranks) of nsteps of the boxes, events on the
+    launching stream, with a barrier and a synchronize on both sides."""
+    torch = D.torch
+    D.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    if fn is None:
+        ctx.step(boxes, nsteps, graph=True)
+    else:
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    D.barrier()
+    return D.max(e0.elapsed_time(e1))
+
+
+def roofline_of(ctx, boxes, cfgs, prof_steps=2):
+    prof = ctx.step_profiled(boxes, prof_steps)
+    launches_per_step = sum(c for _, c in prof.values()) / prof_steps
+    ncell = sum(cells(c) for c in cfgs)
+    kb = {}
+    for cfg in cfgs:
+        for k, v in kernel_bytes_per_cell(cfg).items():
+            kb[k] = kb.get(k, 0.0) + v * cells(cfg)
+    ranked = sorted(((t_ms, k) for k, (t_ms, c) in prof.items() if k in kb), reverse=True)
+    top_ms, top = ranked[0]
+    avg_s = top_ms / 1e3 / prof[top][1]
+    peak, peak_kind = load_peaks()
+    achieved = kb[top] / avg_s / 1e9
+    traffic = NCU_TRAFFIC_BYTES_PER_CELL[top] * ncell if top in NCU_TRAFFIC_BYTES_PER_CELL else None
+    per_kernel = {}
+    for k, (t_ms, c) in prof.items():
+        if c == 0:
+            continue
+        e = {"ms_per_step": round(t_ms / prof_steps, 4), "launches_per_step": c / prof_steps}
+        if k in kb:
+            e["frac_of_peak"] = round(kb[k] / (t_ms / 1e3 / c) / 1e9 / peak, 3)
+        per_kernel[k] = e
+    return {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": f"{peak_kind} copy bandwidth (of measured)",
+            "bytes_per_launch": kb[top], "avg_launch_ms": avg_s * 1e3, "traffic": traffic,
+            "traffic_source": "ncu dram bytes per cell of a 193x384x384 capture, times the cells",
+            "kernel_ms_per_step": {k: v["ms_per_step"] for k, v in per_kernel.items()},
+            "per_kernel": per_kernel}, launches_per_step
+
+
+def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
+    """The same steps through the public C-ABI from pinned host buffers:
+    upload of the initial fields, per step afid_step_graph + the per-box
+    result record (afid_box_get_scalars), download of the final fields."""
+    import ctypes as C
+    torch = D.torch
+    from afid_b200 import _lib
+    from afid_b200.ic import initial_fields
+    L = _lib.lib()
+    fields = ["vx", "vy", "vz", "temp", "pr"]
+    host = []
+    for b, cfg, seed in zip(boxes, cfgs, seeds):
+        f = initial_fields(cfg, b.xc, seed=seed)
+        ins = {}
+        for k in fields:
+            t_in = torch.empty((cfg.nzm, cfg.nym, cfg.nx), dtype=torch.float64, pin_memory=True)
+            t_in.numpy()[...] = f[k].transpose(2, 1, 0)
+            ins[k] = t_in          # the final fields overwrite the initial ones
+        host.append(ins)
+    ids = (C.c_int * len(boxes))(*[b.id for b in boxes])
+    sc = _lib.BoxScalars()
+    h2d = sum(5 * cfg.nx * cfg.nym * cfg.nzm * 8 for cfg in cfgs)
+    torch.cuda.synchronize()
+    D.barrier()
+    t0 = time.perf_counter()
+    for b, ins in zip(boxes, host):
+        for k in fields:
+            _lib.check(L.afid_box_upload(ctx.h, b.id, _lib.FIELDS[k], C.cast(ins[k].data_ptr(), C.POINTER(C.c_double))))
+        _lib.check(L.afid_box_reset(ctx.h, b.id, 0.0))
+    for _ in range(nsteps):
+        _lib.check(L.afid_step_graph(ctx.h, ids, len(boxes), 1))
+        for b in boxes:
+            _lib.check(L.afid_box_get_scalars(ctx.h, b.id, C.byref(sc)))
+    for b, outs in zip(boxes, host):
+        for k in fields:
+            _lib.check(L.afid_box_download(ctx.h, b.id, _lib.FIELDS[k], C.cast(outs[k].data_ptr(), C.POINTER(C.c_double))))
+    t = D.max(time.perf_counter() - t0)
+    ncell = D.sum(sum(cells(c) for c in cfgs))
+    return {"value": ncell * nsteps / t / 1e6, "unit": UNIT,
+            "h2d_bytes_per_step": D.sum(h2d) / nsteps,
+            "d2h_bytes_per_step": D.sum(h2d + C.sizeof(sc) * nsteps * len(boxes)) / nsteps,
+            "what": "afid_box_upload of the initial fields from pinned host memory, K x "
+                    "(afid_step_graph + afid_box_get_scalars of every box), afid_box_download "
+                    "of the final fields"}
+
+
+def serve_record(ctx, D: Dist, rate: float, nreq: int, steps: int, quantum: int = 32) -> dict:
+    """A served stream at ``rate`` requests/s per GPU (nreq per GPU, steps
+    each) with continuous batching, against the plain one-request-at-a-time
+    loop on the same requests; the stream is routed over the ranks."""
+    from afid_b200.serve import plain_split, request_stream, serve, serve_mix, serve_plain, shard_requests
+    torch = D.torch
+    free, _ = torch.cuda.mem_get_info(D.local)
+    budget = int(free * 0.8)
+    mk = lambda: shard_requests(request_stream(nreq * D.world, rate * D.world, seed=2000, steps=steps,
+                                               mix=serve_mix), D.rank, D.world)
+    mine = mk()
+    D.barrier()
+    res_b = serve(ctx, mine, hbm_budget=budget, quantum=quantum)
+    comp_b = [r.finished - r.arrival for r in mine]
+    mine_p = mk()
+    D.barrier()
+    res_p = serve_plain(ctx, mine_p)
+    comp_p = [r.finished - r.arrival for r in mine_p]
+    split = plain_split(mine_p)
+    g = D.gather({"b": res_b, "p": res_p, "cb": comp_b, "cp": comp_p,
+                  "wb": sum(r.cells * r.steps_done for r in mine),
+                  "wp": sum(r.cells * r.steps_done for r in mine_p)})
+
+    def agg(key, comp_key, work_key):
+        span = max(x[key]["makespan_s"] for x in g)
+        comp = np.concatenate([np.array(x[comp_key]) for x in g])
+        d = {"requests": sum(x[key]["requests"] for x in g), "makespan_s": span,
+             "mpoint_steps_s": sum(x[work_key] for x in g) / span / 1e6,
+             "p50_completion_s": float(np.percentile(comp, 50)), "p99_completion_s": float(np.percentile(comp, 99)),
+             "p50_step_latency_ms": max(x[key]["p50_step_latency_ms"] for x in g),
+             "p99_step_latency_ms": max(x[key]["p99_step_latency_ms"] for x in g),
+             "failed": sum(x[key]["failed"] for x in g),
+             "mean_batch": float(np.mean([x[key]["mean_batch"] for x in g]))}
+        return d
+    sb, sp = agg("b", "cb", "wb"), agg("p", "cp", "wp")
+    return {"rate_per_s": rate * D.world, "requests": nreq * D.world, "steps_per_request": steps,
+            "hbm_budget_bytes_per_gpu": budget, "quantum": quantum,
+            "served": sb, "plain": sp, "speedup_vs_plain": sb["mpoint_steps_s"] / sp["mpoint_steps_s"],
+            "plain_split": split if D.world == 1 else None,
+            "mix": "90% ensemble sizes + 10% 193x384x384, Ra log-uniform [1e5,1e9], CFL-adaptive dt"}
+
+
+def c2_record(ctx, stream, D: Dist, steps: int) -> dict:
+    """The plain large box: Mpoint-steps/s over a few steps and the
+    per-kernel HBM roofline, with the built-in launch shapes (the tuner's
+    choices for this size)."""
+    cfg, conf = single_box("c2")
+    boxes = make_boxes(ctx, [cfg], [D.rank])
+    ctx.step(boxes, 2, graph=True)
+    ms = timed_steps(ctx, stream, boxes, steps, D)
+    status = boxes[0].scalars()["status"]
+    roof, _ = roofline_of(ctx, boxes, [cfg])
+    ctx.remove_box(boxes[0])
+    return {"workload": conf["workload"], "steps": steps, "ms_per_step": ms / steps,
+            "value": D.world * cells(cfg) * steps / (ms / 1e3) / 1e6, "status": status, "roofline": roof}
+
+
+# ----------------------------------------------------------------------------
 # GPU arm
 # ----------------------------------------------------------------------------
 def gpu_arm(args):
-    import ctypes as C
-
     import torch
 
-    from afid_b200 import Context, _lib
-    from afid_b200.ic import initial_fields
-
-    rank, world, local = dist_env()
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_
-        from datetime import timedelta
-        dist = dist_
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    device = local
+    from afid_b200 import Context, autotune
+    D = Dist()
+    rank, world, device = D.rank, D.world, D.local
     torch.cuda.set_device(device)
     stream = torch.cuda.Stream(device=device)
     ctx = Context(device)
     ctx.set_stream(stream.cuda_stream)
-    cfgs, conf = workload_boxes(args.workload, rank)
-    boxes = []
-    for q, cfg in enumerate(cfgs):
-        b = ctx.add_box(cfg)
-        f = initial_fields(cfg, b.xc, seed=rank * 1000 + q)
-        for k, v in f.items():
-            b.upload(k, v)
-        boxes.append(b)
-    ncell = sum(cells(c) for c in cfgs)
+    cfgs, seeds, conf, scaling = workload(args.workload, rank, world)
+    boxes = make_boxes(ctx, cfgs, seeds)
+    ncell_rank = sum(cells(c) for c in cfgs)
+    ncell = D.sum(ncell_rank)
 
-    # launch shapes from the autotuner (cached per GPU and size class)
-    from afid_b200 import autotune
     tuned = {}
     if not args.no_tune:
         tuned = autotune.tune(ctx, cfgs)
@@ -291,201 +524,135 @@ def gpu_arm(args):
     ctx.step(boxes, max(args.warmup, 1), graph=True)
     ctx.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
     # ---- timed region: K steps through the captured graph, device events
     clocks = ClockSampler(device)
     clocks.start()
-    barrier()
-    torch.cuda.synchronize(device)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    ctx.step(boxes, args.steps, graph=True)
-    e1.record(stream)
-    torch.cuda.synchronize(device)
-    barrier()
+    ms = timed_steps(ctx, stream, boxes, args.steps, D)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * ncell * args.steps / (ms / 1e3) / 1e6
+    value = ncell * args.steps / (ms / 1e3) / 1e6
     statuses = [b.scalars()["status"] for b in boxes]
+    div_max = max(max(h["divmax"] for h in b.history(args.steps)) for b in boxes)
 
-    # ---- per-kernel device times (CUDA events on the launching stream)
-    prof_steps = 2
-    prof = ctx.step_profiled(boxes, prof_steps)
-    launches_per_step = sum(c for _, c in prof.values()) / prof_steps
-    kb = {}
-    for cfg in cfgs:
-        for k, v in kernel_bytes_per_cell(cfg).items():
-            kb[k] = kb.get(k, 0.0) + v * cells(cfg)
-    ranked = sorted(((t_ms, k) for k, (t_ms, c) in prof.items() if k in kb), reverse=True)
-    top_ms, top = ranked[0]
-    nlaunch = prof[top][1]
-    avg_s = top_ms / 1e3 / nlaunch
-    peak, peak_kind = load_peaks()
-    achieved = kb[top] / avg_s / 1e9
-    traffic = None
-    if top in NCU_TRAFFIC_BYTES_PER_CELL:
-        traffic = NCU_TRAFFIC_BYTES_PER_CELL[top] * ncell
-    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": f"{peak_kind} (copy bandwidth)",
-                "bytes_per_launch": kb[top], "avg_launch_ms": avg_s * 1e3, "traffic": traffic,
-                "kernel_ms_per_step": {k: round(v[0] / prof_steps, 4) for k, v in prof.items()}}
+    roof, launches_per_step = roofline_of(ctx, boxes, cfgs)
+    e2e = e2e_run(ctx, boxes, cfgs, seeds, args.steps, D)
 
-    # ---- end to end through the public C-ABI with pinned host buffers:
-    # upload the initial fields, K steps with the per-step result (plate Nu
-    # record) read back every step, download the final fields.
-    e2e = None
-    if rank == 0 or world > 1:
-        L = _lib.lib()
-        fields = ["vx", "vy", "vz", "temp", "pr"]
-        host_in, host_out = [], []
-        for q, (b, cfg) in enumerate(zip(boxes, cfgs)):
-            f = initial_fields(cfg, b.xc, seed=rank * 1000 + q)
-            ins, outs = {}, {}
-            for k in fields:
-                t_in = torch.empty((cfg.nzm, cfg.nym, cfg.nx), dtype=torch.float64, pin_memory=True)
-                t_in.numpy()[...] = f[k].transpose(2, 1, 0)
-                ins[k] = t_in
-                outs[k] = t_in          # the final fields overwrite the initial ones
-            host_in.append(ins)
-            host_out.append(outs)
-        ids = (C.c_int * len(boxes))(*[b.id for b in boxes])
-        sc = _lib.BoxScalars()
-        h2d = sum(5 * cfg.nx * cfg.nym * cfg.nzm * 8 for cfg in cfgs)
-        torch.cuda.synchronize(device)
-        barrier()
-        t0 = time.perf_counter()
-        for b, ins in zip(boxes, host_in):
-            for k in fields:
-                _lib.check(L.afid_box_upload(ctx.h, b.id, _lib.FIELDS[k],
-                                             C.cast(ins[k].data_ptr(), C.POINTER(C.c_double))))
-            _lib.check(L.afid_box_reset(ctx.h, b.id, 0.0))
-        for _ in range(args.steps):
-            _lib.check(L.afid_step_graph(ctx.h, ids, len(boxes), 1))
-            for b in boxes:
-                _lib.check(L.afid_box_get_scalars(ctx.h, b.id, C.byref(sc)))
-        for b, outs in zip(boxes, host_out):
-            for k in fields:
-                _lib.check(L.afid_box_download(ctx.h, b.id, _lib.FIELDS[k],
-                                               C.cast(outs[k].data_ptr(), C.POINTER(C.c_double))))
-        t_e2e = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([t_e2e], device=f"cuda:{device}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
-        e2e = {"value": world * ncell * args.steps / t_e2e / 1e6, "unit": UNIT,
-               "h2d_bytes_per_step": h2d / args.steps,
-               "d2h_bytes_per_step": (h2d + C.sizeof(sc) * args.steps * len(boxes)) / args.steps,
-               "what": "afid_box_upload of the initial fields from pinned host memory, K x "
-                       "(afid_step_graph + afid_box_get_scalars), afid_box_download of the final fields"}
-
-    # ---- batched against the plain one-box-at-a-time loop (ensemble workload)
     batched = None
     if args.workload == "batch":
-        from afid_b200.ensemble import run_plain, reset_boxes
-        reset_boxes(boxes, seed0=rank * 1000)
-        t_plain = run_plain(ctx, boxes, args.steps, graph=True)
-        batched = {"plain_value": world * ncell * args.steps / t_plain / 1e6,
-                   "plain_ms_per_step": t_plain * 1e3 / args.steps,
-                   "speedup_vs_plain": (world * ncell * args.steps / t_plain / 1e6) and value / (
-                       world * ncell * args.steps / t_plain / 1e6),
-                   "plain": "the same boxes and steps, one box at a time, a CUDA graph per box step"}
+        for b in boxes:                      # capture the one-box graphs outside the timing
+            ctx.step([b], 1, graph=True)
+        reset(boxes, seeds)
+        t_plain = timed_steps(ctx, stream, boxes, args.steps, D,
+                              fn=lambda: [ctx.step([b], args.steps, graph=True) for b in boxes])
+        pv = ncell * args.steps / (t_plain / 1e3) / 1e6
+        batched = {"plain_value": pv, "plain_ms_per_step": t_plain / args.steps,
+                   "speedup_vs_plain": value / pv,
+                   "plain": "the same boxes and steps, one box at a time (a CUDA graph per box "
+                            "step), device time"}
+    for b in boxes:
+        ctx.remove_box(b)
 
-    # ---- CPU baseline (rank 0, N = 1 only)
+    serve_rec = None
+    if args.workload == "batch" and not args.no_serve:
+        serve_rec = serve_record(ctx, D, rate=args.rate, nreq=args.requests, steps=args.serve_steps)
+    c2 = None
+    if args.workload == "batch" and not args.no_c2 and world == 1:
+        c2 = c2_record(ctx, stream, D, steps=5)
+
+    # ---- CPU baseline (rank 0, N = 1): the same workload
     cpu = None
     if world == 1 and not args.no_cpu:
-        v, tps, desc, thr = run_oracle_sample(args.workload, steps=5, warmup=1)
+        csteps = 2 if args.workload == "batch" else 1
+        v, tps = cpu_run(cfgs, seeds, csteps, 0)
+        thr = cpu_threads()
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": f"5 RK3 steps of {desc} with the C/OpenMP restatement of the reference "
-                         f"(oracle/afid_cpu.c, {tps:.2f} s/step on {thr} host threads)"}
+               "sample": f"{csteps} RK3 step(s) of the same {len(cfgs)} box(es) with the C/OpenMP "
+                         f"restatement of the reference (oracle/afid_cpu.c, {tps:.2f} s/step on "
+                         f"{thr} host threads)"}
 
     if rank == 0:
         conf = dict(conf)
-        field_mb = ncell * 8 / 1e6   # one field of all boxes of a rank
-        l2 = ("inputs larger than L2 (each field %.0f MB, 9 resident fields >> 126 MB), no flush" % field_mb
-              if 9 * field_mb > 2 * 126 else
-              "inputs fit in L2 (each field %.1f MB), no flush: a small-box latency measurement, "
-              "not a bandwidth one" % field_mb)
-        conf.update({"global_batch": len(cfgs) * world, "parallelism": f"replicas x{world}",
-                     "l2": l2, "graph": "one CUDA graph per step", "grid": "istr3=7 Chebyshev-Gauss-Lobatto"})
+        field_mb = ncell_rank * 8 / 1e6   # one field of all boxes of a rank
+        conf.update({
+            "global_batch": len(cfgs) * world if args.workload != "batch" else conf["boxes"],
+            "l2": ("inputs larger than L2 (each field %.0f MB per GPU, 9 resident fields), no flush"
+                   % field_mb if field_mb > 126 else
+                   "inputs fit in L2 (each field %.1f MB), no flush: a latency measurement" % field_mb),
+            "graph": "one CUDA graph per step", "grid": "istr3=7 Chebyshev-Gauss-Lobatto",
+            "div_resid": DIV_RESID})
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC_BATCH if args.workload == "batch" else METRIC_BOX,
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": conf, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "scaling": scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": conf, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)), "clocks": clk,
-            "status": statuses,
+            "status": statuses, "max_divergence_timed": div_max,
         }
         if batched is not None:
             line["batched"] = batched
+        if serve_rec is not None:
+            line["serve"] = serve_rec
+        if c2 is not None:
+            line["c2"] = c2
         if tuned:
             line["tuning"] = {k: {q: v[q] for q in ("fft_y_lines", "fft_z_lines", "k1_minb")}
                               for k, v in tuned.items()}
         print(json.dumps(line), flush=True)
     ctx.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    D.close()
     return 0
 
 
 def serve_arm(args):
-    """Served stream: Poisson arrivals at each rate, continuous batching
-    against the plain one-request-at-a-time loop."""
+    """Served stream at each rate against the plain loop (one line)."""
     import torch
 
     from afid_b200 import Context
-    from afid_b200.serve import request_stream, serve, serve_mix, serve_plain
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    ctx = Context(local)
-    free, total = torch.cuda.mem_get_info(local)
-    budget = int(free * 0.8)
+    D = Dist()
+    torch.cuda.set_device(D.local)
+    ctx = Context(D.local)
     out = {}
     for rate in args.rates:
-        reqs = request_stream(args.requests, rate, seed=2000 + rank, steps=args.serve_steps, mix=serve_mix)
-        res_b = serve(ctx, reqs, hbm_budget=budget, quantum=32)
-        reqs = request_stream(args.requests, rate, seed=2000 + rank, steps=args.serve_steps, mix=serve_mix)
-        res_p = serve_plain(ctx, reqs)
-        out[str(rate)] = {"served": res_b, "plain": res_p,
-                          "speedup_vs_plain": res_b["mpoint_steps_s"] / res_p["mpoint_steps_s"]}
+        out[str(rate)] = serve_record(ctx, D, rate=rate, nreq=args.requests, steps=args.serve_steps)
     ctx.close()
-    if rank == 0:
+    if D.rank == 0:
         best = max(out.values(), key=lambda d: d["served"]["mpoint_steps_s"])
-        line = {"metric": METRIC + "; served stream", "value": best["served"]["mpoint_steps_s"],
-                "unit": UNIT, "n_gpus": world, "steps": args.serve_steps, "warmup": 0,
+        line = {"metric": METRIC_BATCH + "; served stream sweep", "value": best["served"]["mpoint_steps_s"],
+                "unit": UNIT, "n_gpus": D.world, "steps": args.serve_steps, "warmup": 0,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded Poisson arrivals)",
-                "config": {"workload": f"served stream, {args.requests} requests per rate, "
+                "config": {"workload": f"served stream, {args.requests} requests per GPU per rate, "
                                        f"{args.serve_steps} CFL-adaptive steps each, 90% ensemble sizes + "
-                                       "10% 193x384x384, Ra log-uniform [1e5,1e9]",
-                           "hbm_budget_bytes": budget},
+                                       "10% 193x384x384, Ra log-uniform [1e5,1e9]"},
                 "rates": out}
         print(json.dumps(line), flush=True)
+    D.close()
     return 0
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "s384", "batch"])
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="batch", choices=["batch", "c1", "c2", "c3", "s384"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
-    ap.add_argument("--serve", action="store_true", help="run the served-stream benchmark")
-    ap.add_argument("--rates", type=float, nargs="+", default=[10.0, 100.0])
-    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream sub-record")
+    ap.add_argument("--no-c2", action="store_true", help="skip the large-box sub-record")
+    ap.add_argument("--rate", type=float, default=50.0, help="arrivals/s of the serve sub-record")
+    ap.add_argument("--serve", action="store_true", help="run the served-stream sweep over --rates")
+    ap.add_argument("--rates", type=float, nargs="+", default=[1.0, 10.0, 50.0, 200.0])
+    ap.add_argument("--requests", type=int, default=32, help="requests per GPU of a served stream")
     ap.add_argument("--serve-steps", type=int, default=200)
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU through torch.distributed.run
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+               f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+               "--master-port", str(free_port()), os.path.abspath(__file__)] + sys.argv[1:]
+        return subprocess.call(cmd)
     if args.impl == "reference":
         return reference_arm(args)
     if args.serve:
