@@ -11,6 +11,9 @@ kernel (afid_step_profiled), and keeps the fastest:
   with two x-planes per barrier; 32x4 tiles with 4, 5 or 6 blocks; 32x2
   tiles with 8 blocks.
 
+``tune`` tunes each size class on a box of its own (for single boxes);
+``tune_batch`` tunes a set of boxes that are stepped together, on the set.
+
 Results do not depend on the shapes (tests/test_gpu_batch.py checks batched
 against single-box results bit for bit), so tuning is purely a speed choice.
 The choices are cached in a JSON file keyed by GPU name and size class.
@@ -156,6 +159,49 @@ def tune(ctx, cfgs, cache: TuneCache | None = None, steps: int = 2) -> dict:
     except OSError:
         pass
     return out
+
+
+def tune_batch(ctx, boxes, steps: int = 2) -> dict:
+    """Tune the launch shapes of a set of boxes stepped together: each
+    candidate is applied to every box of the set (where it is valid for the
+    box) and the set's own kernel times decide.  Shapes that are best for a
+    box alone are not best in a batch: a transform launch takes the largest
+    tile of its boxes, so one class asking for big tiles lowers the
+    occupancy of all.  Returns the chosen values and their times; the boxes
+    keep the chosen shapes."""
+    y_all = sorted({v for b in boxes for v in candidates(b.cfg)["fft_y_lines"]})
+    z_all = sorted({v for b in boxes for v in candidates(b.cfg)["fft_z_lines"]})
+
+    def set_all(fy, fz, mb):
+        for b in boxes:
+            c = candidates(b.cfg)
+            b.set_tuning(fy if fy in c["fft_y_lines"] else 0, fz if fz in c["fft_z_lines"] else 0, mb)
+
+    def t(kernels):
+        ctx.step(boxes, 1)
+        prof = ctx.step_profiled(boxes, steps)
+        return sum(prof[k][0] for k in kernels) / steps
+
+    res = {}
+    set_all(0, 0, 0)
+    res[("y", 0)] = t(("fft_y_fwd", "fft_y_inv"))
+    for fy in y_all:
+        set_all(fy, 0, 0)
+        res[("y", fy)] = t(("fft_y_fwd", "fft_y_inv"))
+    fy = min([0] + y_all, key=lambda v: res[("y", v)])
+    set_all(fy, 0, 0)
+    res[("z", 0)] = t(("fft_z_fwd", "fft_z_inv"))
+    for fz in z_all:
+        set_all(fy, fz, 0)
+        res[("z", fz)] = t(("fft_z_fwd", "fft_z_inv"))
+    fz = min([0] + z_all, key=lambda v: res[("z", v)])
+    for mb in candidates(boxes[0].cfg)["k1_minb"]:
+        set_all(fy, fz, mb)
+        res[("k1", mb)] = t(("explicit_fwd",))
+    mb = min(candidates(boxes[0].cfg)["k1_minb"], key=lambda v: res[("k1", v)])
+    set_all(fy, fz, mb)
+    return {"fft_y_lines": fy, "fft_z_lines": fz, "k1_minb": mb,
+            "ms_per_step": {f"{a}{b}": round(v, 4) for (a, b), v in res.items()}}
 
 
 def apply(box, choices: dict):

@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libafid_gpu.so")
 SOURCES = ["afid_capi.cu"]
-HEADERS = ["afid_device.cuh", "k_stencil.cuh", "k_fft.cuh", "k_routine.cuh"]
+HEADERS = ["afid_device.cuh", "k_stencil.cuh", "k_fft.cuh", "k_fftw.cuh", "k_routine.cuh"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

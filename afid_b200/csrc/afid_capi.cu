@@ -7,12 +7,14 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
 
 #include "afid_device.cuh"
 #include "k_fft.cuh"
+#include "k_fftw.cuh"
 #include "k_routine.cuh"
 #include "k_stencil.cuh"
 #include "../../include/afid_gpu.h"
@@ -47,8 +49,12 @@ int fail(int code, const char *fmt, ...) {
       return fail(AFID_ECUDA, "launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); \
   } while (0)
 
-// Launch families; each has its own table of tile offsets per batch.
-enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, FAM_K2, NFAM };
+// Launch families; each has its own table of tile offsets per batch.  The
+// y transforms of boxes with a warp plan run in FAM_WY8/16/24 (values per
+// lane), the others in FAM_FY.
+enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, FAM_K2,
+           FAM_WY8, FAM_WY16, FAM_WY24, NFAM };
+constexpr int WY_V[3] = {8, 16, 24};
 constexpr int HIST_CAP = 4096;
 
 struct HostBox {
@@ -74,6 +80,8 @@ struct Batch {
   FftSmem sm_y{0, 0}, sm_z{0, 0};   // slot and twiddle sizes of the persistent transforms
   int grid_y = 0, grid_z = 0;       // their resident grids
   int k2_block = 256;               // threads per block of the back-substitution kernel
+  size_t smem_wy[3] = {};           // shared memory and resident grids of the warp y transforms
+  int grid_wy[3] = {};
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
   int k1_minb = 4;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
@@ -101,6 +109,55 @@ int factor_radices(int n, int *rad, int *np) {
   return 0;
 }
 
+// Warp plan of an n-point transform (k_fftw.cuh): V values per lane (8, 16
+// or 24), G = n / V lanes per line (a power of two <= 32), and a radix
+// sequence whose radices all divide V, power-of-two radices first; the
+// fewest passes win, then the fewer values per lane.  Returns 0 (no plan)
+// for sizes the tile kernels keep: lines longer than WARP_PLAN_MAX_N, where
+// the tile kernels measured faster (384 and 768 points).
+constexpr int WARP_PLAN_MAX_N = 128;
+int warp_plan(int n, int *v_out, int *g_out, int *rad, int *np) {
+  static const int cand[7] = {16, 12, 8, 6, 4, 3, 2};
+  if (n > WARP_PLAN_MAX_N) return 0;
+  int best_v = 0, best_np = 99, best[8] = {};
+  for (int vi = 0; vi < 3; ++vi) {
+    const int V = WY_V[vi];
+    if (n % V) continue;
+    const int G = n / V;
+    if (G > 32 || (G & (G - 1))) continue;
+    // depth-first search for the shortest factorisation into radices dividing V
+    int cur[8], found[8] = {}, found_np = 99;
+    std::function<void(int, int)> dfs = [&](int m, int d) {
+      if (d >= found_np || d >= 8) return;
+      if (m == 1) {
+        found_np = d;
+        for (int q = 0; q < d; ++q) found[q] = cur[q];
+        return;
+      }
+      for (int c : cand)
+        if (V % c == 0 && m % c == 0) {
+          cur[d] = c;
+          dfs(m / c, d + 1);
+        }
+    };
+    dfs(n, 0);
+    if (found_np < best_np) {
+      best_np = found_np;
+      best_v = V;
+      for (int q = 0; q < found_np; ++q) best[q] = found[q];
+    }
+  }
+  if (!best_v) return 0;
+  // power-of-two radices first (shift-and-mask indexing of the strides)
+  int o = 0;
+  for (int q = 0; q < best_np; ++q) if ((best[q] & (best[q] - 1)) == 0) rad[o++] = best[q];
+  for (int q = 0; q < best_np; ++q) if ((best[q] & (best[q] - 1)) != 0) rad[o++] = best[q];
+  *v_out = best_v;
+  *g_out = n / best_v;
+  *np = best_np;
+  return 1;
+}
+
 // Variants of the explicit/forward kernel: tile height TI (block of 32 TI
 // threads), resident blocks per SM and planes per barrier.
 //   2: 32x8 tiles, 2 blocks/SM        3: 32x8 tiles, 3 blocks/SM (80 registers)
@@ -119,7 +176,9 @@ long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 
     case FAM_COL: return cdiv(B.plane, 256);
     case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
     case FAM_DIAG: return cdiv(B.plane, 256);
-    case FAM_FY: return (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
+    case FAM_FY: return B.wy_v ? 0 : (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
+    case FAM_WY8: case FAM_WY16: case FAM_WY24:
+      return B.wy_v == WY_V[fam - FAM_WY8] ? cdiv((long long)B.nxm * wy_units_per_plane(B), WF_WARPS) : 0;
     case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
     case FAM_PX: return cdiv(px_pairs(B.nzm, B.nymh), 256);
   }
@@ -339,6 +398,7 @@ int get_box(afid_ctx *c, int id, HostBox **out) {
 }
 
 int init_kernel_attrs();
+int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid);
 
 
 // slot sizes (complex values) and twiddle lengths of the persistent
@@ -452,10 +512,62 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     int rc = init_kernel_attrs();
     if (!rc) rc = fft_grid(k_fft_y_fwd, bt->smem_y, bt->total[FAM_FY], &bt->grid_y);
     if (!rc) rc = fft_grid(k_fft_z<-1>, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
+    if (!rc) rc = wy_shapes(devs, bt->total, bt->smem_wy, bt->grid_wy);
     if (rc) { free_batch(bt); return rc; }
   }
   c->batches[key] = bt;
   *out = bt;
+  return 0;
+}
+
+// Shared memory (largest y size of each class) and resident grid of the
+// warp y transforms of a set of boxes.
+int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid) {
+  for (int c = 0; c < 3; ++c) {
+    int nmax = 0;
+    for (const BoxDev &d : devs)
+      if (d.wy_v == WY_V[c]) nmax = std::max(nmax, d.nym);
+    smem[c] = nmax ? wf_smem_bytes(nmax, WY_V[c]) : 0;
+    grid[c] = 0;
+    if (!total[FAM_WY8 + c]) continue;
+    int dev = 0, nsm = 0, occ = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    switch (c) {
+      case 0: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, WF_T, smem[c])); break;
+      case 1: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<16>, WF_T, smem[c])); break;
+      default: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<24>, WF_T, smem[c])); break;
+    }
+    if (occ < 1) return fail(AFID_ESIZE, "warp transform block of %zu bytes does not fit an SM", smem[c]);
+    grid[c] = std::max(1, std::min(total[FAM_WY8 + c], nsm * occ));
+  }
+  return 0;
+}
+
+// The y transforms of a batch: the tile kernel for boxes without a warp
+// plan, one warp-kernel launch per values-per-lane class present.
+template <class BD>
+int launch_fft_y(bool fwd, const int *total, BD bd, int grid_y, size_t smem_y, FftSmem sm_y, const int *grid_wy,
+                 const size_t *smem_wy, cudaStream_t s, int ns) {
+  if (total[FAM_FY] > 0) {
+    if (fwd) k_fft_y_fwd<<<grid_y, FFT_T, smem_y, s>>>(bd(FAM_FY), ns, sm_y, total[FAM_FY]);
+    else k_fft_y_inv<<<grid_y, FFT_T, smem_y, s>>>(bd(FAM_FY), ns, sm_y, total[FAM_FY]);
+    CKL();
+  }
+  for (int c = 0; c < 3; ++c) {
+    const int f = FAM_WY8 + c;
+    if (!total[f]) continue;
+    const BatchDev b = bd(f);
+    switch (c) {
+      case 0: if (fwd) k_fftw_y_fwd<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+              else k_fftw_y_inv<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]); break;
+      case 1: if (fwd) k_fftw_y_fwd<16><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+              else k_fftw_y_inv<16><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]); break;
+      default: if (fwd) k_fftw_y_fwd<24><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+               else k_fftw_y_inv<24><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]); break;
+    }
+    CKL();
+  }
   return 0;
 }
 
@@ -487,6 +599,12 @@ int init_kernel_attrs() {
   CK(cudaFuncSetAttribute(k_fft_y_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_fwd<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_fwd<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_fwd<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_inv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_inv<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_inv<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   done[dev] = true;
   return 0;
 }
@@ -533,8 +651,11 @@ int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof 
     CKL();
     PMARK(pf, AFID_K_DIVERGENCE);
   }
-  k_fft_y_fwd<<<bt->grid_y, FFT_T, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns, bt->sm_y, bt->total[FAM_FY]);
-  CKL();
+  {
+    int rc = launch_fft_y(true, bt->total, [&](int f) { return bdev(bt, f); }, bt->grid_y, bt->smem_y, bt->sm_y,
+                          bt->grid_wy, bt->smem_wy, s, ns);
+    if (rc) return rc;
+  }
   PMARK(pf, AFID_K_FFT_Y_FWD);
   k_fft_z<-1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
@@ -547,8 +668,11 @@ int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof 
   k_fft_z<+1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
   CKL();
   PMARK(pf, AFID_K_FFT_Z_INV);
-  k_fft_y_inv<<<bt->grid_y, FFT_T, bt->smem_y, s>>>(bdev(bt, FAM_FY), ns, bt->sm_y, bt->total[FAM_FY]);
-  CKL();
+  {
+    int rc = launch_fft_y(false, bt->total, [&](int f) { return bdev(bt, f); }, bt->grid_y, bt->smem_y, bt->sm_y,
+                          bt->grid_wy, bt->smem_wy, s, ns);
+    if (rc) return rc;
+  }
   PMARK(pf, AFID_K_FFT_Y_INV);
   return 0;
 }
@@ -781,6 +905,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
     delete hb;
     return fail(AFID_EFFT, "FFT size not efficient: nym=%d nzm=%d need prime factors <= 7 (code 444)", p->nym, p->nzm);
   }
+  if (!warp_plan(d.nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np)) d.wy_v = 0;
   Sizes s = sizes_of(*p);
   d.plane = s.plane; d.fsize = s.fsize; d.nspec = s.nspec;
   d.dx = (double)p->nxm / p->alx3; d.dy = (double)p->nym / p->ylen; d.dz = (double)p->nzm / p->zlen;
@@ -1702,6 +1827,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   memset(&d, 0, sizeof d);
   if (factor_radices(nym, d.fft_y_radix, &d.fft_y_np) || factor_radices(nzm, d.fft_z_radix, &d.fft_z_np))
     return fail(AFID_EFFT, "noalloc: nym=%d nzm=%d need prime factors <= 7", nym, nzm);
+  if (!warp_plan(nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np)) d.wy_v = 0;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   int rc = noalloc_setup(dev);
@@ -1788,7 +1914,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   static_assert(sizeof(off) <= 16 * sizeof(double), "tile tables exceed their scratch slot");
   for (int f = 0; f < NFAM; ++f) {
     off[f][0] = 0;
-    off[f][1] = total[f] = (f == FAM_FY || f == FAM_FZ || f == FAM_PX) ? (int)tiles_of(d, f) : 0;
+    off[f][1] = total[f] = (f == FAM_FY || f == FAM_FZ || f == FAM_PX || f >= FAM_WY8) ? (int)tiles_of(d, f) : 0;
   }
   CK(cudaMemcpyAsync(base + o_tab, tab, (size_t)n_tab * 8, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(base + o_tw, g_noalloc_host.tw, (size_t)(nym + nzm) * 16, cudaMemcpyHostToDevice, st));
@@ -1804,22 +1930,25 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   fft_smem_grow(d, smy, smz, twy, twz);
   const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + FFT_TAIL_BYTES;
   const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + FFT_TAIL_BYTES;
+  size_t swy[3];
+  int gwy[3];
   rc = fft_grid(k_fft_y_fwd, sy, total[FAM_FY], &gy);
   if (!rc) rc = fft_grid(k_fft_z<-1>, sz, total[FAM_FZ], &gz);
+  if (!rc) rc = wy_shapes(std::vector<BoxDev>{d}, total, swy, gwy);
   if (rc) return rc;
   // the x-solve's pivots, for this call's grid
   k_poisson_pivots<<<(unsigned)cdiv(px_pairs(nzm, d.nymh), 256), 256, 0, st>>>(d);
   CKL();
-  k_fft_y_fwd<<<gy, FFT_T, sy, st>>>(bd(FAM_FY), 0, smy, total[FAM_FY]);
-  CKL();
+  rc = launch_fft_y(true, total, bd, gy, sy, smy, gwy, swy, st, 0);
+  if (rc) return rc;
   k_fft_z<-1><<<gz, FFT_T, sz, st>>>(bd(FAM_FZ), 0, smz, total[FAM_FZ]);
   CKL();
   rc = launch_poisson_x(total, bd, st, 0);
   if (rc) return rc;
   k_fft_z<+1><<<gz, FFT_T, sz, st>>>(bd(FAM_FZ), 0, smz, total[FAM_FZ]);
   CKL();
-  k_fft_y_inv<<<gy, FFT_T, sy, st>>>(bd(FAM_FY), 0, smy, total[FAM_FY]);
-  CKL();
+  rc = launch_fft_y(false, total, bd, gy, sy, smy, gwy, swy, st, 0);
+  if (rc) return rc;
   if (status) {
     // wait for this call's kernels and report its status word
     int v = -1;

@@ -111,6 +111,10 @@ struct BoxDev {
   int fz_rb;            // kz rows per TMA box of the z transform (a divisor of nzm, <= 256)
   const CUtensorMap *tm_z;  // TMA map of spec as a 2-D FP64 array (2*nymh x nxm*nzm), box 2L x fz_rb
   int piv_ready;        // 1 = dstore holds the Poisson pivots of this grid
+  // warp-transform plan of the y transforms (k_fftw.cuh): wy_v values per
+  // lane (0: no plan, the tile kernels run), wy_g lanes per line, radices
+  int wy_v, wy_g, wy_np;
+  int wy_rad[8];
   // test switch of the bounded waits (afid_box_test_skip_z_copies): the z
   // transform arms its slot mbarriers without issuing the box's tile copies,
   // and its waits give up after mbar_tries polls (0: MBAR_MAX_TRIES)

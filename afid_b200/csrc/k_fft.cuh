@@ -42,6 +42,18 @@ __device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, doub
   a3 = csub(t1, wt3);
 }
 
+// three-point DFT in place: X[k] = sum_n a_n W3^(n k), W3 = exp(SGN 2 pi i / 3)
+template <int SGN>
+__device__ __forceinline__ void dft3(double2 &a0, double2 &a1, double2 &a2) {
+  constexpr double S3 = 0.86602540378443864676;   // sin(2 pi / 3)
+  const double2 s = cadd(a1, a2), d = csub(a1, a2);
+  const double2 m = make_double2(a0.x - 0.5 * s.x, a0.y - 0.5 * s.y);
+  const double2 id = make_double2((-SGN * S3) * d.y, (SGN * S3) * d.x);
+  a0 = cadd(a0, s);
+  a1 = cadd(m, id);
+  a2 = csub(m, id);
+}
+
 template <int R, int SGN>
 __device__ __forceinline__ void dft_small(double2 (&v)[R], const double2 *tw, int N) {
   constexpr double H = 0.70710678118654752440;    // cos(pi/4)
@@ -94,14 +106,42 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], const double2 *tw, in
     t = v[7]; v[7] = v[13]; v[13] = t;
     t = v[11]; v[11] = v[14]; v[14] = t;
   } else if constexpr (R == 3) {
-    const double S3 = 0.86602540378443864676;   // sin(2 pi / 3)
-    const double2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    const double2 a0 = v[0];
-    const double2 m = make_double2(a0.x - 0.5 * s.x, a0.y - 0.5 * s.y);
-    const double2 id = make_double2((-SGN * S3) * d.y, (SGN * S3) * d.x);
-    v[0] = cadd(a0, s);
-    v[1] = cadd(m, id);
-    v[2] = csub(m, id);
+    dft3<SGN>(v[0], v[1], v[2]);
+  } else if constexpr (R == 6) {
+    // 6 = 2 x 3: three-point DFTs of the even and odd samples, then
+    // X[k] = E[k] + W6^k O[k], X[k+3] = E[k] - W6^k O[k]
+    constexpr double S3 = 0.86602540378443864676;   // sin(pi / 3)
+    double2 e0 = v[0], e1 = v[2], e2 = v[4], o0 = v[1], o1 = v[3], o2 = v[5];
+    dft3<SGN>(e0, e1, e2);
+    dft3<SGN>(o0, o1, o2);
+    o1 = cmul_wi<SGN>(o1, 0.5, S3);     // W6^1
+    o2 = cmul_wi<SGN>(o2, -0.5, S3);    // W6^2
+    v[0] = cadd(e0, o0); v[3] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[4] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[5] = csub(e2, o2);
+  } else if constexpr (R == 12) {
+    // 12 = 3 x 4: four-point DFTs over n2 of x[n1 + 3 n2] (Y[n1][k2] kept in
+    // slot n1 + 3 k2), twiddle by W12^(n1 k2), three-point DFTs over n1
+    // (X[k2 + 4 k1] lands in slot 3 k2 + k1), then a register renaming into
+    // natural order
+    constexpr double S3 = 0.86602540378443864676;   // sin(pi / 3) = cos(pi / 6)
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) dft4<SGN>(v[n1], v[n1 + 3], v[n1 + 6], v[n1 + 9]);
+    v[4] = cmul_wi<SGN>(v[4], S3, 0.5);      // n1=1 k2=1: W12^1
+    v[7] = cmul_wi<SGN>(v[7], 0.5, S3);      // n1=1 k2=2: W12^2
+    v[10] = mul_sgn_i<SGN>(v[10]);           // n1=1 k2=3: W12^3
+    v[5] = cmul_wi<SGN>(v[5], 0.5, S3);      // n1=2 k2=1: W12^2
+    v[8] = cmul_wi<SGN>(v[8], -0.5, S3);     // n1=2 k2=2: W12^4
+    v[11] = make_double2(-v[11].x, -v[11].y);  // n1=2 k2=3: W12^6
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) dft3<SGN>(v[3 * k2], v[3 * k2 + 1], v[3 * k2 + 2]);
+    double2 t[12];
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+      for (int k1 = 0; k1 < 3; ++k1) t[k2 + 4 * k1] = v[3 * k2 + k1];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) v[q] = t[q];
   } else if constexpr (R == 5) {
     const double C1 = 0.30901699437494742410, C2 = -0.80901699437494742410;
     const double S1 = 0.95105651629515357212, S2 = 0.58778525229247312917;

@@ -1,0 +1,238 @@
+// Warp transforms along y (the r2c and c2r steps of
+// SolvePressureCorrection.F90:97 and :148).
+//
+// Each warp transforms LPW = 32 / G complex lines of length N on its own:
+// G lanes per line, V = N / G values per lane.  The plan is a mixed-radix
+// Stockham sequence whose radices all divide V, so in every pass each lane
+// computes exactly V / R butterflies of radix R (no idle lanes).  Passes
+// exchange data through the warp's own shared-memory region (LPW lines x N
+// values, interleaved n * LPW + line) with __syncwarp only: warps never wait
+// for each other.  The first pass of the forward transform loads its
+// butterflies' inputs straight from HBM (two real rows per complex line, the
+// lanes of a line reading consecutive values); the last pass of the inverse
+// transform stores straight to HBM.
+//
+// Block structure: 8 warps; a block tile is 8 consecutive warp units (LPW
+// lines each) of one box.  Persistent blocks take runs of block tiles
+// round-robin (as the other transforms) and keep the box descriptor and the
+// twiddle table of their current box in shared memory, reloading both (with
+// the block's only barriers) when the box changes.
+#pragma once
+#include "k_fft.cuh"
+
+namespace afid {
+
+constexpr int WF_WARPS = 8;            // warps per block
+constexpr int WF_T = 32 * WF_WARPS;    // threads per block
+
+// lines per warp and values per lane of box B's y plan
+__host__ __device__ __forceinline__ int wy_lpw(const BoxDev &B) { return 32 / B.wy_g; }
+
+// warp units of a box: LPW complex lines = 2 LPW rows of one plane
+__host__ __device__ __forceinline__ int wy_units_per_plane(const BoxDev &B) {
+  return (B.nzm + 2 * wy_lpw(B) - 1) / (2 * wy_lpw(B));
+}
+
+// One Stockham pass of radix R over the warp's LPW lines (lane: line
+// lane % LPW, butterflies j = lane / LPW + b G for b < V / R).
+template <int R, int SGN, int V, class Src, class Dst>
+__device__ __forceinline__ void wpass(int N, int lgL, int Ns, const double2 *tw, const Src &src, const Dst &dst) {
+  constexpr int BPT = V / R;
+  const int lane = threadIdx.x & 31;
+  const int NR = N / R, tstr = N / (Ns * R);
+  const FastDiv dNs(Ns);
+  const int l = lane & ((1 << lgL) - 1), j0 = lane >> lgL, jstep = 32 >> lgL;
+  double2 v[BPT][R];
+#pragma unroll
+  for (int b = 0; b < BPT; ++b) {
+    const int j = j0 + b * jstep;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b][r] = src(l, j + r * NR);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < BPT; ++b) {
+    const int j = j0 + b * jstep;
+    const int k = dNs.mod(j);
+    if (Ns > 1) twiddle<R, SGN>(v[b], k, tstr, tw);
+    dft_small<R, SGN>(v[b], tw, N);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst(l, base + r * Ns, v[b][r]);
+  }
+  __syncwarp();
+}
+
+template <int SGN, int V, class Src, class Dst>
+__device__ __forceinline__ void wrun(int R, int N, int lgL, int Ns, const double2 *tw, const Src &src, const Dst &dst) {
+  // only the radices that divide V occur in a plan with V values per lane
+  switch (R) {
+    case 2: if constexpr (V % 2 == 0) wpass<2, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+    case 3: if constexpr (V % 3 == 0) wpass<3, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+    case 4: if constexpr (V % 4 == 0) wpass<4, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+    case 6: if constexpr (V % 6 == 0) wpass<6, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+    case 8: if constexpr (V % 8 == 0) wpass<8, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+    case 12: if constexpr (V % 12 == 0) wpass<12, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+    default: if constexpr (V % 16 == 0) wpass<16, SGN, V>(N, lgL, Ns, tw, src, dst); break;
+  }
+}
+
+// The warp's whole transform: the first pass reads src, the last writes dst
+// (the passes between go through the warp's region a).
+template <int SGN, int V, class Src, class Dst>
+__device__ __forceinline__ void wfft(double2 *a, int N, int lgL, const int *rad, int np, const double2 *tw,
+                                     const Src &src, const Dst &dst) {
+  const SmemSrc as{a, lgL};
+  const SmemDst ad{a, lgL};
+  if (np == 1) {
+    wrun<SGN, V>(rad[0], N, lgL, 1, tw, src, dst);
+    return;
+  }
+  wrun<SGN, V>(rad[0], N, lgL, 1, tw, src, ad);
+  int Ns = rad[0];
+  for (int p = 1; p < np - 1; ++p) {
+    wrun<SGN, V>(rad[p], N, lgL, Ns, tw, as, ad);
+    Ns *= rad[p];
+  }
+  wrun<SGN, V>(rad[np - 1], N, lgL, Ns, tw, as, dst);
+}
+
+// first pass of the forward transform: line p = rows (2p, 2p+1) of the
+// unit, read from HBM (rows beyond nzm are zero)
+struct WRowPairSrc {
+  const double *rows;   // row 2p of line p at rows + 2 p N
+  int N, nrow;          // rows present in the unit
+  __device__ __forceinline__ double2 operator()(int p, int n) const {
+    const double a = 2 * p < nrow ? __ldcg(rows + (long long)(2 * p) * N + n) : 0.0;
+    const double b = 2 * p + 1 < nrow ? __ldcg(rows + (long long)(2 * p + 1) * N + n) : 0.0;
+    return make_double2(a, b);
+  }
+};
+
+// shared-memory layout of a warp-transform block: the twiddles (N complex),
+// the mbarrier-free tail (box descriptor), then one region per warp
+__host__ __device__ __forceinline__ int wf_region(int N, int V) { return 32 * V; (void)N; }
+__host__ __device__ __forceinline__ size_t wf_smem_bytes(int N, int V) {
+  return (size_t)N * 16 + FFT_DESC_BYTES + (size_t)WF_WARPS * 32 * V * 16;
+}
+
+// Block tile t_local of box B: warp w takes unit t_local * 8 + w.
+template <int V>
+__global__ void __launch_bounds__(WF_T, 2) k_fftw_y_fwd(BatchDev bt, int ns, int total) {
+  extern __shared__ double2 wsm[];
+  BoxDev &sb = *reinterpret_cast<BoxDev *>(wsm);            // descriptor of the current box
+  double2 *tws = wsm + FFT_DESC_BYTES / 16;                  // its twiddles
+  double2 *reg = nullptr;                                    // this warp's region (set per box)
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const TileRange rg(total);
+  if (rg.first() >= total) return;
+  TileWalk wk(bt, rg.first());
+  int loaded = -1;
+  bool run = false;
+  for (int t = rg.first(); t < total; t = rg.next(t)) {
+    const int lt = wk.to(bt, t);
+    if (wk.b != loaded) {
+      __syncthreads();
+      fft_load_box(bt, wk.b, sb);
+      __syncthreads();
+      for (int q = threadIdx.x; q < sb.nym; q += WF_T) tws[q] = __ldg(sb.twy + q);
+      loaded = wk.b;
+      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
+      reg = tws + sb.nym + w * 32 * V;
+    }
+    if (!run) continue;
+    const BoxDev &B = sb;
+    const int N = B.nym, nzm = B.nzm, nh = B.nymh, lpw = wy_lpw(B), lgL = ilog2(lpw);
+    const int upp = wy_units_per_plane(B);
+    const int u = lt * WF_WARPS + w;
+    if (u >= B.nxm * upp) continue;
+    const int k = u / upp, i0 = (u - k * upp) * 2 * lpw;
+    const int nrow = min(2 * lpw, nzm - i0);
+    const double *rows = B.phi + (long long)k * B.plane + (long long)i0 * N;
+    wfft<-1, V>(reg, N, lgL, B.wy_rad, B.wy_np, tws, WRowPairSrc{rows, N, nrow}, SmemDst{reg, lgL});
+    // unpack the two real transforms of line p: A = (Z_q + conj Z_{N-q}) / 2,
+    // B = (Z_q - conj Z_{N-q}) / (2i), q <= N/2
+    const int l = lane & (lpw - 1), g = 32 / lpw;
+    double2 *const speck = B.spec + (long long)k * nzm * nh;
+    const int i = i0 + 2 * l;
+    for (int q = lane >> lgL; q < nh; q += g) {
+      const double2 z = reg[sidx(l, q, lgL)];
+      const double2 zn = reg[sidx(l, q == 0 ? 0 : N - q, lgL)];
+      const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
+      const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
+      if (i < nzm) __stcg(speck + (long long)i * nh + q, A);
+      if (i + 1 < nzm) __stcg(speck + (long long)(i + 1) * nh + q, Bv);
+    }
+    __syncwarp();
+  }
+}
+
+// first pass of the inverse transform: line p = the complex line
+// A + i B of the half-spectrum rows (2p, 2p+1), read from HBM with the
+// Hermitian extension (the imaginary parts at ky = 0 and ky = N/2 ignored,
+// as in a c2r transform)
+struct WHalfPairSrc {
+  const double2 *rows;  // row 2p of line p at rows + 2 p nh
+  int N, nh, nrow;
+  __device__ __forceinline__ double2 coef(int r, int n) const {
+    if (r >= nrow) return make_double2(0.0, 0.0);
+    const int q = n < nh ? n : N - n;
+    double2 c = __ldcg(rows + (long long)r * nh + q);
+    if (q == 0 || 2 * q == N) c.y = 0.0;
+    else if (n >= nh) c.y = -c.y;
+    return c;
+  }
+  __device__ __forceinline__ double2 operator()(int p, int n) const {
+    const double2 A = coef(2 * p, n), Bv = coef(2 * p + 1, n);
+    return make_double2(A.x - Bv.y, A.y + Bv.x);
+  }
+};
+// last pass of the inverse transform: the real and imaginary parts are the
+// two output rows, stored to HBM
+struct WRowPairDst {
+  double *rows;
+  int N, nrow;
+  __device__ __forceinline__ void operator()(int p, int n, double2 v) const {
+    if (2 * p < nrow) __stcg(rows + (long long)(2 * p) * N + n, v.x);
+    if (2 * p + 1 < nrow) __stcg(rows + (long long)(2 * p + 1) * N + n, v.y);
+  }
+};
+
+template <int V>
+__global__ void __launch_bounds__(WF_T, 2) k_fftw_y_inv(BatchDev bt, int ns, int total) {
+  extern __shared__ double2 wsm[];
+  BoxDev &sb = *reinterpret_cast<BoxDev *>(wsm);
+  double2 *tws = wsm + FFT_DESC_BYTES / 16;
+  double2 *reg = nullptr;
+  const int w = threadIdx.x >> 5;
+  const TileRange rg(total);
+  if (rg.first() >= total) return;
+  TileWalk wk(bt, rg.first());
+  int loaded = -1;
+  bool run = false;
+  for (int t = rg.first(); t < total; t = rg.next(t)) {
+    const int lt = wk.to(bt, t);
+    if (wk.b != loaded) {
+      __syncthreads();
+      fft_load_box(bt, wk.b, sb);
+      __syncthreads();
+      for (int q = threadIdx.x; q < sb.nym; q += WF_T) tws[q] = __ldg(sb.twy + q);
+      loaded = wk.b;
+      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
+      reg = tws + sb.nym + w * 32 * V;
+    }
+    if (!run) continue;
+    const BoxDev &B = sb;
+    const int N = B.nym, nzm = B.nzm, nh = B.nymh, lpw = wy_lpw(B), lgL = ilog2(lpw);
+    const int upp = wy_units_per_plane(B);
+    const int u = lt * WF_WARPS + w;
+    if (u >= B.nxm * upp) continue;
+    const int k = u / upp, i0 = (u - k * upp) * 2 * lpw;
+    const int nrow = min(2 * lpw, nzm - i0);
+    const double2 *half = B.spec + (long long)k * nzm * nh + (long long)i0 * nh;
+    double *rows = B.phi + (long long)k * B.plane + (long long)i0 * N;
+    wfft<+1, V>(reg, N, lgL, B.wy_rad, B.wy_np, tws, WHalfPairSrc{half, N, nh, nrow}, WRowPairDst{rows, N, nrow});
+  }
+}
+
+}  // namespace afid

@@ -516,9 +516,12 @@ def gpu_arm(args):
 
     tuned = {}
     if not args.no_tune:
-        tuned = autotune.tune(ctx, cfgs)
-        for b in boxes:
-            autotune.apply(b, tuned)
+        if len(boxes) > 1:
+            tuned = {"batch": autotune.tune_batch(ctx, boxes)}
+        else:
+            tuned = autotune.tune(ctx, cfgs)
+            for b in boxes:
+                autotune.apply(b, tuned)
 
     # warm-up (also captures the CUDA graph of one step)
     ctx.step(boxes, max(args.warmup, 1), graph=True)
@@ -538,6 +541,10 @@ def gpu_arm(args):
 
     batched = None
     if args.workload == "batch":
+        if not args.no_tune:                 # each box alone runs its own class's best shapes
+            per_class = autotune.tune(ctx, cfgs)
+            for b in boxes:
+                autotune.apply(b, per_class)
         for b in boxes:                      # capture the one-box graphs outside the timing
             ctx.step([b], 1, graph=True)
         reset(boxes, seeds)
@@ -547,7 +554,8 @@ def gpu_arm(args):
         batched = {"plain_value": pv, "plain_ms_per_step": t_plain / args.steps,
                    "speedup_vs_plain": value / pv,
                    "plain": "the same boxes and steps, one box at a time (a CUDA graph per box "
-                            "step), device time"}
+                            "step, each box with the launch shapes tuned for its size class), "
+                            "device time"}
     for b in boxes:
         ctx.remove_box(b)
 

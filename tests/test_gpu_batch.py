@@ -112,3 +112,24 @@ def test_launch_shapes_do_not_change_results(ctx, fy, fz, k1):
             b.set_tuning(**bad)
     for x in (a, b):
         ctx.remove_box(x)
+
+
+def test_batch_tuning_keeps_results(ctx):
+    """autotune.tune_batch chooses the launch shapes on the set itself; the
+    chosen shapes change no result bit."""
+    from afid_b200 import autotune
+    tuned = [_add(ctx, kw, 20 + q) for q, kw in enumerate(MIX)]
+    plain = [_add(ctx, kw, 20 + q) for q, kw in enumerate(MIX)]
+    choice = autotune.tune_batch(ctx, tuned, steps=1)
+    assert choice["k1_minb"] in autotune.candidates(tuned[0].cfg)["k1_minb"]
+    for b, kw, q in zip(tuned, MIX, range(len(MIX))):        # restart from the seeded state
+        for k, v in initial_fields(b.cfg, b.xc, 20 + q).items():
+            b.upload(k, v)
+        b.reset(b.cfg.dt)
+    ctx.step(tuned, 2, graph=True)
+    ctx.step(plain, 2, graph=True)
+    for a, b in zip(tuned, plain):
+        for f in FIELDS:
+            assert np.array_equal(a.download(f), b.download(f)), f
+    for b in tuned + plain:
+        ctx.remove_box(b)
