@@ -115,7 +115,7 @@ int factor_radices(int n, int *rad, int *np) {
 // fewest passes win, then the fewer values per lane.  Returns 0 (no plan)
 // for sizes the tile kernels keep: lines longer than WARP_PLAN_MAX_N, where
 // the tile kernels measured faster (384 and 768 points).
-constexpr int WARP_PLAN_MAX_N = 128;
+constexpr int WARP_PLAN_MAX_N = WF_MAX_N;
 int warp_plan(int n, int *v_out, int *g_out, int *rad, int *np) {
   static const int cand[7] = {16, 12, 8, 6, 4, 3, 2};
   if (n > WARP_PLAN_MAX_N) return 0;
@@ -178,7 +178,7 @@ long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 
     case FAM_DIAG: return cdiv(B.plane, 256);
     case FAM_FY: return B.wy_v ? 0 : (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
     case FAM_WY8: case FAM_WY16: case FAM_WY24:
-      return B.wy_v == WY_V[fam - FAM_WY8] ? cdiv((long long)B.nxm * wy_units_per_plane(B), WF_WARPS) : 0;
+      return B.wy_v == WY_V[fam - FAM_WY8] ? (long long)B.nxm * wy_units_per_plane(B) : 0;
     case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
     case FAM_PX: return cdiv(px_pairs(B.nzm, B.nymh), 256);
   }
@@ -520,14 +520,12 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   return 0;
 }
 
-// Shared memory (largest y size of each class) and resident grid of the
-// warp y transforms of a set of boxes.
+// Shared memory and resident grid (in blocks of WF_WARPS warps, at most
+// one warp per unit) of the warp y transforms of a set of boxes.
 int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid) {
+  (void)devs;
   for (int c = 0; c < 3; ++c) {
-    int nmax = 0;
-    for (const BoxDev &d : devs)
-      if (d.wy_v == WY_V[c]) nmax = std::max(nmax, d.nym);
-    smem[c] = nmax ? wf_smem_bytes(nmax, WY_V[c]) : 0;
+    smem[c] = wf_smem_bytes(WY_V[c]);
     grid[c] = 0;
     if (!total[FAM_WY8 + c]) continue;
     int dev = 0, nsm = 0, occ = 0;
@@ -539,7 +537,7 @@ int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, i
       default: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<24>, WF_T, smem[c])); break;
     }
     if (occ < 1) return fail(AFID_ESIZE, "warp transform block of %zu bytes does not fit an SM", smem[c]);
-    grid[c] = std::max(1, std::min(total[FAM_WY8 + c], nsm * occ));
+    grid[c] = std::max(1, std::min((int)cdiv(total[FAM_WY8 + c], WF_WARPS), nsm * occ));
   }
   return 0;
 }
@@ -708,7 +706,7 @@ int launch_substep(const Batch *bt, cudaStream_t s, int ns, Prof *pf = nullptr) 
 
 int launch_step(const Batch *bt, cudaStream_t s, Prof *pf = nullptr) {
   const int nb = (int)bt->ids.size();
-  k_diag<<<bt->total[FAM_DIAG], 256, 0, s>>>(bdev(bt, FAM_DIAG));
+  k_diag<<<bt->total[FAM_DIAG], 256, 0, s>>>(bdev(bt, FAM_DIAG), 0);
   CKL();
   PMARK(pf, AFID_K_DIAG);
   k_finalize<<<cdiv(nb, 128), 128, 0, s>>>(bt->d_boxes, nb, 0);
@@ -1413,7 +1411,7 @@ static int diag_now(afid_ctx *c, int id, BoxScalars *bs) {
   if (rc) return rc;
   void *red = (char *)hb->dev.sc + offsetof(BoxScalars, red_u64);
   CK(cudaMemsetAsync(red, 0, sizeof(bs->red_u64), c->stream));
-  k_diag<<<bt->total[FAM_DIAG], 256, 0, c->stream>>>(bdev(bt, FAM_DIAG));
+  k_diag<<<bt->total[FAM_DIAG], 256, 0, c->stream>>>(bdev(bt, FAM_DIAG), 1);
   CKL();
   CK(cudaMemcpyAsync(bs, hb->dev.sc, sizeof(BoxScalars), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemsetAsync(red, 0, sizeof(bs->red_u64), c->stream));

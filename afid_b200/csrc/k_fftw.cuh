@@ -12,11 +12,13 @@
 // lanes of a line reading consecutive values); the last pass of the inverse
 // transform stores straight to HBM.
 //
-// Block structure: 8 warps; a block tile is 8 consecutive warp units (LPW
-// lines each) of one box.  Persistent blocks take runs of block tiles
-// round-robin (as the other transforms) and keep the box descriptor and the
-// twiddle table of their current box in shared memory, reloading both (with
-// the block's only barriers) when the box changes.
+// Warps are independent: a warp unit is LPW lines (2 LPW rows of one plane)
+// of one box, the units of a launch are numbered across its boxes, and each
+// warp of the (persistent) grid takes runs of WF_RUN consecutive units,
+// the runs dealt round-robin over all warps.  A warp keeps the fields of its
+// current box in registers and that box's twiddles and radices in its own
+// slice of shared memory, reloading them (with __syncwarp only) when its
+// unit belongs to another box: a block has no barrier at all.
 #pragma once
 #include "k_fft.cuh"
 
@@ -24,14 +26,65 @@ namespace afid {
 
 constexpr int WF_WARPS = 8;            // warps per block
 constexpr int WF_T = 32 * WF_WARPS;    // threads per block
+constexpr int WF_RUN = 4;              // consecutive units per run of a warp
+constexpr int WF_MAX_N = 128;          // longest line with a warp plan
 
-// lines per warp and values per lane of box B's y plan
+// lines per warp and units per plane of box B's y plan
 __host__ __device__ __forceinline__ int wy_lpw(const BoxDev &B) { return 32 / B.wy_g; }
-
-// warp units of a box: LPW complex lines = 2 LPW rows of one plane
 __host__ __device__ __forceinline__ int wy_units_per_plane(const BoxDev &B) {
   return (B.nzm + 2 * wy_lpw(B) - 1) / (2 * wy_lpw(B));
 }
+
+// a warp's slice of shared memory: twiddles (WF_MAX_N complex), radices
+// (8 ints, 32 bytes), then the work region (32 V complex)
+__host__ __device__ __forceinline__ int wf_slice(int V) { return WF_MAX_N + 2 + 32 * V; }   // complex values
+__host__ __device__ __forceinline__ size_t wf_smem_bytes(int V) { return (size_t)WF_WARPS * wf_slice(V) * 16; }
+
+// The unit sequence of a warp: runs gw, gw + W, gw + 2W, ... of WF_RUN
+// units (gw: the warp's index in the grid, W: the grid's warps).
+struct WarpUnits {
+  int gw, nw, total;
+  __device__ __forceinline__ explicit WarpUnits(int total_)
+      : gw((int)(blockIdx.x * WF_WARPS + (threadIdx.x >> 5))), nw((int)(gridDim.x * WF_WARPS)), total(total_) {}
+  __device__ __forceinline__ int first() const { return gw * WF_RUN < total ? gw * WF_RUN : total; }
+  __device__ __forceinline__ int next(int u) const {
+    int n = u + 1;
+    if (n % WF_RUN == 0) n = (u / WF_RUN + nw) * WF_RUN;
+    return n < total ? n : total;
+  }
+};
+
+// The fields of a box a warp transform needs, held in registers; load()
+// also copies the box's twiddles and radices into the warp's slice.
+struct WarpBox {
+  int b, N, nzm, nh, nxm, lpw, lgL, upp, np;
+  long long plane;
+  double *phi;
+  double2 *spec;
+  bool run;
+  __device__ __forceinline__ void load(const BatchDev &bt, int bi, int ns, double2 *tws, int *rad) {
+    const BoxDev *Bp = bt.boxes + bi;
+    b = bi;
+    N = __ldg(&Bp->nym);
+    nzm = __ldg(&Bp->nzm);
+    nh = __ldg(&Bp->nymh);
+    nxm = __ldg(&Bp->nxm);
+    lpw = 32 / __ldg(&Bp->wy_g);
+    lgL = ilog2(lpw);
+    upp = (nzm + 2 * lpw - 1) / (2 * lpw);
+    np = __ldg(&Bp->wy_np);
+    plane = __ldg(&Bp->plane);
+    phi = (double *)__ldg((const unsigned long long *)&Bp->phi);
+    spec = (double2 *)__ldg((const unsigned long long *)&Bp->spec);
+    const double2 *twy = (const double2 *)__ldg((const unsigned long long *)&Bp->twy);
+    run = __ldg(&Bp->active) && ns < __ldg(&Bp->nsst) &&
+          *(volatile int *)&((BoxScalars *)__ldg((const unsigned long long *)&Bp->sc))->status == 0;
+    const int lane = threadIdx.x & 31;
+    for (int q = lane; q < N; q += 32) tws[q] = __ldg(twy + q);
+    if (lane < 8) rad[lane] = __ldg(&Bp->wy_rad[lane]);
+    __syncwarp();
+  }
+};
 
 // One Stockham pass of radix R over the warp's LPW lines (lane: line
 // lane % LPW, butterflies j = lane / LPW + b G for b < V / R).
@@ -109,59 +162,41 @@ struct WRowPairSrc {
   }
 };
 
-// shared-memory layout of a warp-transform block: the twiddles (N complex),
-// the mbarrier-free tail (box descriptor), then one region per warp
-__host__ __device__ __forceinline__ int wf_region(int N, int V) { return 32 * V; (void)N; }
-__host__ __device__ __forceinline__ size_t wf_smem_bytes(int N, int V) {
-  return (size_t)N * 16 + FFT_DESC_BYTES + (size_t)WF_WARPS * 32 * V * 16;
-}
 
-// Block tile t_local of box B: warp w takes unit t_local * 8 + w.
+// Forward (r2c) y transform of the units of the launch.
 template <int V>
 __global__ void __launch_bounds__(WF_T, 2) k_fftw_y_fwd(BatchDev bt, int ns, int total) {
   extern __shared__ double2 wsm[];
-  BoxDev &sb = *reinterpret_cast<BoxDev *>(wsm);            // descriptor of the current box
-  double2 *tws = wsm + FFT_DESC_BYTES / 16;                  // its twiddles
-  double2 *reg = nullptr;                                    // this warp's region (set per box)
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const TileRange rg(total);
-  if (rg.first() >= total) return;
-  TileWalk wk(bt, rg.first());
-  int loaded = -1;
-  bool run = false;
-  for (int t = rg.first(); t < total; t = rg.next(t)) {
-    const int lt = wk.to(bt, t);
-    if (wk.b != loaded) {
-      __syncthreads();
-      fft_load_box(bt, wk.b, sb);
-      __syncthreads();
-      for (int q = threadIdx.x; q < sb.nym; q += WF_T) tws[q] = __ldg(sb.twy + q);
-      loaded = wk.b;
-      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
-      reg = tws + sb.nym + w * 32 * V;
-    }
-    if (!run) continue;
-    const BoxDev &B = sb;
-    const int N = B.nym, nzm = B.nzm, nh = B.nymh, lpw = wy_lpw(B), lgL = ilog2(lpw);
-    const int upp = wy_units_per_plane(B);
-    const int u = lt * WF_WARPS + w;
-    if (u >= B.nxm * upp) continue;
-    const int k = u / upp, i0 = (u - k * upp) * 2 * lpw;
-    const int nrow = min(2 * lpw, nzm - i0);
-    const double *rows = B.phi + (long long)k * B.plane + (long long)i0 * N;
-    wfft<-1, V>(reg, N, lgL, B.wy_rad, B.wy_np, tws, WRowPairSrc{rows, N, nrow}, SmemDst{reg, lgL});
-    // unpack the two real transforms of line p: A = (Z_q + conj Z_{N-q}) / 2,
+  double2 *const tws = wsm + (threadIdx.x >> 5) * wf_slice(V);   // this warp's slice
+  int *const rad = reinterpret_cast<int *>(tws + WF_MAX_N);
+  double2 *const reg = tws + WF_MAX_N + 2;
+  const int lane = threadIdx.x & 31;
+  const WarpUnits wu(total);
+  if (wu.first() >= total) return;
+  TileWalk wk(bt, wu.first());
+  WarpBox X;
+  X.b = -1;
+  for (int u = wu.first(); u < total; u = wu.next(u)) {
+    const int lu = wk.to(bt, u);
+    if (wk.b != X.b) X.load(bt, wk.b, ns, tws, rad);
+    if (!X.run) continue;
+    const int N = X.N, lpw = X.lpw, lgL = X.lgL;
+    const int k = lu / X.upp, i0 = (lu - k * X.upp) * 2 * lpw;
+    const int nrow = min(2 * lpw, X.nzm - i0);
+    const double *rows = X.phi + (long long)k * X.plane + (long long)i0 * N;
+    wfft<-1, V>(reg, N, lgL, rad, X.np, tws, WRowPairSrc{rows, N, nrow}, SmemDst{reg, lgL});
+    // unpack the two real transforms of line l: A = (Z_q + conj Z_{N-q}) / 2,
     // B = (Z_q - conj Z_{N-q}) / (2i), q <= N/2
-    const int l = lane & (lpw - 1), g = 32 / lpw;
-    double2 *const speck = B.spec + (long long)k * nzm * nh;
+    const int l = lane & (lpw - 1), g = 32 / lpw, nh = X.nh;
+    double2 *const speck = X.spec + (long long)k * X.nzm * nh;
     const int i = i0 + 2 * l;
     for (int q = lane >> lgL; q < nh; q += g) {
       const double2 z = reg[sidx(l, q, lgL)];
       const double2 zn = reg[sidx(l, q == 0 ? 0 : N - q, lgL)];
       const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
       const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
-      if (i < nzm) __stcg(speck + (long long)i * nh + q, A);
-      if (i + 1 < nzm) __stcg(speck + (long long)(i + 1) * nh + q, Bv);
+      if (i < X.nzm) __stcg(speck + (long long)i * nh + q, A);
+      if (i + 1 < X.nzm) __stcg(speck + (long long)(i + 1) * nh + q, Bv);
     }
     __syncwarp();
   }
@@ -198,40 +233,28 @@ struct WRowPairDst {
   }
 };
 
+// Inverse (c2r) y transform of the units of the launch.
 template <int V>
 __global__ void __launch_bounds__(WF_T, 2) k_fftw_y_inv(BatchDev bt, int ns, int total) {
   extern __shared__ double2 wsm[];
-  BoxDev &sb = *reinterpret_cast<BoxDev *>(wsm);
-  double2 *tws = wsm + FFT_DESC_BYTES / 16;
-  double2 *reg = nullptr;
-  const int w = threadIdx.x >> 5;
-  const TileRange rg(total);
-  if (rg.first() >= total) return;
-  TileWalk wk(bt, rg.first());
-  int loaded = -1;
-  bool run = false;
-  for (int t = rg.first(); t < total; t = rg.next(t)) {
-    const int lt = wk.to(bt, t);
-    if (wk.b != loaded) {
-      __syncthreads();
-      fft_load_box(bt, wk.b, sb);
-      __syncthreads();
-      for (int q = threadIdx.x; q < sb.nym; q += WF_T) tws[q] = __ldg(sb.twy + q);
-      loaded = wk.b;
-      run = __syncthreads_and(sb.active && ns < sb.nsst && *(volatile int *)&sb.sc->status == 0);
-      reg = tws + sb.nym + w * 32 * V;
-    }
-    if (!run) continue;
-    const BoxDev &B = sb;
-    const int N = B.nym, nzm = B.nzm, nh = B.nymh, lpw = wy_lpw(B), lgL = ilog2(lpw);
-    const int upp = wy_units_per_plane(B);
-    const int u = lt * WF_WARPS + w;
-    if (u >= B.nxm * upp) continue;
-    const int k = u / upp, i0 = (u - k * upp) * 2 * lpw;
-    const int nrow = min(2 * lpw, nzm - i0);
-    const double2 *half = B.spec + (long long)k * nzm * nh + (long long)i0 * nh;
-    double *rows = B.phi + (long long)k * B.plane + (long long)i0 * N;
-    wfft<+1, V>(reg, N, lgL, B.wy_rad, B.wy_np, tws, WHalfPairSrc{half, N, nh, nrow}, WRowPairDst{rows, N, nrow});
+  double2 *const tws = wsm + (threadIdx.x >> 5) * wf_slice(V);
+  int *const rad = reinterpret_cast<int *>(tws + WF_MAX_N);
+  double2 *const reg = tws + WF_MAX_N + 2;
+  const WarpUnits wu(total);
+  if (wu.first() >= total) return;
+  TileWalk wk(bt, wu.first());
+  WarpBox X;
+  X.b = -1;
+  for (int u = wu.first(); u < total; u = wu.next(u)) {
+    const int lu = wk.to(bt, u);
+    if (wk.b != X.b) X.load(bt, wk.b, ns, tws, rad);
+    if (!X.run) continue;
+    const int N = X.N, lpw = X.lpw, lgL = X.lgL, nh = X.nh;
+    const int k = lu / X.upp, i0 = (lu - k * X.upp) * 2 * lpw;
+    const int nrow = min(2 * lpw, X.nzm - i0);
+    const double2 *half = X.spec + (long long)k * X.nzm * nh + (long long)i0 * nh;
+    double *rows = X.phi + (long long)k * X.plane + (long long)i0 * N;
+    wfft<+1, V>(reg, N, lgL, rad, X.np, tws, WHalfPairSrc{half, N, nh, nrow}, WRowPairDst{rows, N, nrow});
   }
 }
 

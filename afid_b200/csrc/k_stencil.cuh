@@ -744,13 +744,15 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 // Column march as in k_divergence: one thread per (j, i); vx(k+1) of one
-// plane is vx(k) of the next, so every field is read once.
-__global__ void __launch_bounds__(256, 2) k_diag(BatchDev bt) {
+// plane is vx(k) of the next, so every field is read once.  In a step
+// (every_box = 0) a failed or held box is skipped; the routine-level calls
+// (CalcMaxCFL, CheckDivergence) evaluate the box whatever its status.
+__global__ void __launch_bounds__(256, 2) k_diag(BatchDev bt, int every_box) {
   const int b = find_box(bt.tile_off, bt.nbox, blockIdx.x);
   const BoxDev &B = bt.boxes[b];
   if (!B.active) return;
   BoxScalars *S = B.sc;
-  if (S->status != 0) return;
+  if (!every_box && S->status != 0) return;
   const long long P = B.plane;
   const long long col = (long long)(blockIdx.x - __ldg(bt.tile_off + b)) * blockDim.x + threadIdx.x;
   double cfl = 0.0, dv = 0.0, my = 0.0, mz = 0.0;

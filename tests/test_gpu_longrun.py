@@ -28,11 +28,13 @@ def test_long_run_mean_nu_within_one_percent(ctx, tmp_path):
     cpu = wnus_means(z["nu_vol"], z["nu_bot"], z["nu_top"])
     for k in gpu:
         assert abs(gpu[k] - cpu[k]) <= 0.01 * abs(cpu[k]), (k, gpu[k], cpu[k])
-    assert max(res["divmax"]) <= 1e-10
+    # CheckDivergence at the output times, on the held box
+    assert 0.0 < max(res["divmax"]) <= 1e-10
+    assert max(res["cfl"]) > 1e-8
     # the log files carry the same series (nu_plate.out at its 6 digits)
     plate = np.loadtxt(tmp_path / "nu_plate.out")
     vol = np.loadtxt(tmp_path / "nu_vol.out")
     assert plate.shape == (len(z["time"]), 3) and vol.shape == (len(z["time"]), 2)
-    assert np.allclose(plate[:, 1], res["nu_bot"], rtol=1e-6, atol=0)
+    assert np.allclose(plate[:, 1], res["nu_bot"], rtol=1e-5, atol=0)
     assert np.array_equal(vol[:, 1], res["nu_vol"])
     ctx.remove_box(box)
