@@ -50,11 +50,12 @@ int fail(int code, const char *fmt, ...) {
   } while (0)
 
 // Launch families; each has its own table of tile offsets per batch.  The
-// y transforms of boxes with a warp plan run in FAM_WY8/16/24 (values per
+// y transforms of boxes with a warp plan run in FAM_WY8/12 (values per
 // lane), the others in FAM_FY.
 enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, FAM_K2,
-           FAM_WY8, FAM_WY16, FAM_WY24, NFAM };
-constexpr int WY_V[3] = {8, 16, 24};
+           FAM_WY8, FAM_WY12, NFAM };
+constexpr int WY_NV = 2;
+constexpr int WY_V[WY_NV] = {8, 12};
 constexpr int HIST_CAP = 4096;
 
 struct HostBox {
@@ -80,8 +81,8 @@ struct Batch {
   FftSmem sm_y{0, 0}, sm_z{0, 0};   // slot and twiddle sizes of the persistent transforms
   int grid_y = 0, grid_z = 0;       // their resident grids
   int k2_block = 256;               // threads per block of the back-substitution kernel
-  size_t smem_wy[3] = {};           // shared memory and resident grids of the warp y transforms
-  int grid_wy[3] = {};
+  size_t smem_wy[WY_NV] = {};       // shared memory and resident grids of the warp y transforms
+  int grid_wy[WY_NV] = {};
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
   int k1_minb = 4;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
@@ -109,18 +110,19 @@ int factor_radices(int n, int *rad, int *np) {
   return 0;
 }
 
-// Warp plan of an n-point transform (k_fftw.cuh): V values per lane (8, 16
-// or 24), G = n / V lanes per line (a power of two <= 32), and a radix
-// sequence whose radices all divide V, power-of-two radices first; the
-// fewest passes win, then the fewer values per lane.  Returns 0 (no plan)
-// for sizes the tile kernels keep: lines longer than WARP_PLAN_MAX_N, where
-// the tile kernels measured faster (384 and 768 points).
+// Warp plan of an n-point transform (k_fftw.cuh): V values per lane (8 or
+// 12; 16 and 24 spilled registers at two blocks per SM), G = n / V lanes per
+// line (a power of two <= 32), and a radix sequence whose radices all divide
+// V, power-of-two radices first; the fewest passes win, then the fewer
+// values per lane.  Returns 0 (no plan) for sizes the tile kernels keep:
+// lines longer than WARP_PLAN_MAX_N, where the tile kernels measured faster
+// (384 and 768 points).
 constexpr int WARP_PLAN_MAX_N = WF_MAX_N;
 int warp_plan(int n, int *v_out, int *g_out, int *rad, int *np) {
   static const int cand[7] = {16, 12, 8, 6, 4, 3, 2};
   if (n > WARP_PLAN_MAX_N) return 0;
   int best_v = 0, best_np = 99, best[8] = {};
-  for (int vi = 0; vi < 3; ++vi) {
+  for (int vi = 0; vi < WY_NV; ++vi) {
     const int V = WY_V[vi];
     if (n % V) continue;
     const int G = n / V;
@@ -177,7 +179,7 @@ long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 
     case FAM_CELL: return cdiv((long long)B.nxm * B.plane, 256);
     case FAM_DIAG: return cdiv(B.plane, 256);
     case FAM_FY: return B.wy_v ? 0 : (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
-    case FAM_WY8: case FAM_WY16: case FAM_WY24:
+    case FAM_WY8: case FAM_WY12:
       return B.wy_v == WY_V[fam - FAM_WY8] ? (long long)B.nxm * wy_units_per_plane(B) : 0;
     case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
     case FAM_PX: return cdiv(px_pairs(B.nzm, B.nymh), 256);
@@ -524,18 +526,15 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
 // one warp per unit) of the warp y transforms of a set of boxes.
 int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid) {
   (void)devs;
-  for (int c = 0; c < 3; ++c) {
+  for (int c = 0; c < WY_NV; ++c) {
     smem[c] = wf_smem_bytes(WY_V[c]);
     grid[c] = 0;
     if (!total[FAM_WY8 + c]) continue;
     int dev = 0, nsm = 0, occ = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    switch (c) {
-      case 0: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, WF_T, smem[c])); break;
-      case 1: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<16>, WF_T, smem[c])); break;
-      default: CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<24>, WF_T, smem[c])); break;
-    }
+    if (c == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, WF_T, smem[c]));
+    else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<12>, WF_T, smem[c]));
     if (occ < 1) return fail(AFID_ESIZE, "warp transform block of %zu bytes does not fit an SM", smem[c]);
     grid[c] = std::max(1, std::min((int)cdiv(total[FAM_WY8 + c], WF_WARPS), nsm * occ));
   }
@@ -552,17 +551,16 @@ int launch_fft_y(bool fwd, const int *total, BD bd, int grid_y, size_t smem_y, F
     else k_fft_y_inv<<<grid_y, FFT_T, smem_y, s>>>(bd(FAM_FY), ns, sm_y, total[FAM_FY]);
     CKL();
   }
-  for (int c = 0; c < 3; ++c) {
+  for (int c = 0; c < WY_NV; ++c) {
     const int f = FAM_WY8 + c;
     if (!total[f]) continue;
     const BatchDev b = bd(f);
-    switch (c) {
-      case 0: if (fwd) k_fftw_y_fwd<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
-              else k_fftw_y_inv<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]); break;
-      case 1: if (fwd) k_fftw_y_fwd<16><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
-              else k_fftw_y_inv<16><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]); break;
-      default: if (fwd) k_fftw_y_fwd<24><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
-               else k_fftw_y_inv<24><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]); break;
+    if (c == 0) {
+      if (fwd) k_fftw_y_fwd<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+      else k_fftw_y_inv<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+    } else {
+      if (fwd) k_fftw_y_fwd<12><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+      else k_fftw_y_inv<12><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
     }
     CKL();
   }
@@ -598,11 +596,9 @@ int init_kernel_attrs() {
   CK(cudaFuncSetAttribute(k_fft_z<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fft_z<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fftw_y_fwd<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  CK(cudaFuncSetAttribute(k_fftw_y_fwd<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  CK(cudaFuncSetAttribute(k_fftw_y_fwd<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_fwd<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fftw_y_inv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  CK(cudaFuncSetAttribute(k_fftw_y_inv<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
-  CK(cudaFuncSetAttribute(k_fftw_y_inv<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_y_inv<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   done[dev] = true;
   return 0;
 }
@@ -1928,8 +1924,8 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   fft_smem_grow(d, smy, smz, twy, twz);
   const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + FFT_TAIL_BYTES;
   const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + FFT_TAIL_BYTES;
-  size_t swy[3];
-  int gwy[3];
+  size_t swy[WY_NV];
+  int gwy[WY_NV];
   rc = fft_grid(k_fft_y_fwd, sy, total[FAM_FY], &gy);
   if (!rc) rc = fft_grid(k_fft_z<-1>, sz, total[FAM_FZ], &gz);
   if (!rc) rc = wy_shapes(std::vector<BoxDev>{d}, total, swy, gwy);

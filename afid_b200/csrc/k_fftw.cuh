@@ -2,7 +2,7 @@
 // SolvePressureCorrection.F90:97 and :148).
 //
 // Each warp transforms LPW = 32 / G complex lines of length N on its own:
-// G lanes per line, V = N / G values per lane.  The plan is a mixed-radix
+// G lanes per line, V = N / G values per lane (8 or 12).  The plan is a mixed-radix
 // Stockham sequence whose radices all divide V, so in every pass each lane
 // computes exactly V / R butterflies of radix R (no idle lanes).  Passes
 // exchange data through the warp's own shared-memory region (LPW lines x N
