@@ -51,9 +51,10 @@ int fail(int code, const char *fmt, ...) {
 
 // Launch families; each has its own table of tile offsets per batch.  The
 // y transforms of boxes with a warp plan run in FAM_WY8/12 (values per
-// lane), the others in FAM_FY.
+// lane), the others in FAM_FY; likewise the z transforms in FAM_WZ8/12 and
+// FAM_FZ.
 enum Fam { FAM_K1 = 0, FAM_COL, FAM_CELL, FAM_DIAG, FAM_FY, FAM_FZ, FAM_PX, FAM_K2,
-           FAM_WY8, FAM_WY12, NFAM };
+           FAM_WY8, FAM_WY12, FAM_WZ8, FAM_WZ12, NFAM };
 constexpr int WY_NV = 2;
 constexpr int WY_V[WY_NV] = {8, 12};
 constexpr int HIST_CAP = 4096;
@@ -83,6 +84,7 @@ struct Batch {
   int k2_block = 256;               // threads per block of the back-substitution kernel
   size_t smem_wy[WY_NV] = {};       // shared memory and resident grids of the warp y transforms
   int grid_wy[WY_NV] = {};
+  int grid_wz[WY_NV] = {};          // resident grids of the warp z transforms (shared memory as y)
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
   int k1_minb = 4;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
@@ -181,7 +183,9 @@ long long tiles_of(const BoxDev &B, int fam, int k1_variant = 2, int k2_block = 
     case FAM_FY: return B.wy_v ? 0 : (long long)B.nxm * cdiv(B.nzm, 2 * fft_y_pairs(B));
     case FAM_WY8: case FAM_WY12:
       return B.wy_v == WY_V[fam - FAM_WY8] ? (long long)B.nxm * wy_units_per_plane(B) : 0;
-    case FAM_FZ: return (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
+    case FAM_FZ: return B.wz_v ? 0 : (long long)B.nxm * cdiv(B.nymh, fft_z_lines(B));
+    case FAM_WZ8: case FAM_WZ12:
+      return B.wz_v == WY_V[fam - FAM_WZ8] ? (long long)B.nxm * wz_units_per_plane(B) : 0;
     case FAM_PX: return cdiv(px_pairs(B.nzm, B.nymh), 256);
   }
   return 0;
@@ -400,19 +404,22 @@ int get_box(afid_ctx *c, int id, HostBox **out) {
 }
 
 int init_kernel_attrs();
-int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid);
+int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid, int *grid_z);
 
 
 // slot sizes (complex values) and twiddle lengths of the persistent
-// transforms, grown to cover box d
+// transforms, grown to cover box d (the directions d runs in a tile kernel)
 void fft_smem_grow(const BoxDev &d, FftSmem &y, FftSmem &z, int &twy, int &twz) {
-  const int Pp = fft_y_pairs(d), L = fft_z_lines(d);
-  y.slot = std::max(y.slot, fft_y_slot(d.nym, Pp));
-  z.slot = std::max(z.slot, L * d.nzm);
-  y.tw = std::max(y.tw, d.nym);
-  z.tw = std::max(z.tw, d.nzm);
-  twy = std::max(twy, d.nym);
-  twz = std::max(twz, d.nzm);
+  if (!d.wy_v) {
+    y.slot = std::max(y.slot, fft_y_slot(d.nym, fft_y_pairs(d)));
+    y.tw = std::max(y.tw, d.nym);
+    twy = std::max(twy, d.nym);
+  }
+  if (!d.wz_v) {
+    z.slot = std::max(z.slot, fft_z_lines(d) * d.nzm);
+    z.tw = std::max(z.tw, d.nzm);
+    twz = std::max(twz, d.nzm);
+  }
 }
 
 // resident grid of a persistent transform: SMs x blocks per SM, at most tiles
@@ -514,7 +521,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     int rc = init_kernel_attrs();
     if (!rc) rc = fft_grid(k_fft_y_fwd, bt->smem_y, bt->total[FAM_FY], &bt->grid_y);
     if (!rc) rc = fft_grid(k_fft_z<-1>, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
-    if (!rc) rc = wy_shapes(devs, bt->total, bt->smem_wy, bt->grid_wy);
+    if (!rc) rc = wy_shapes(devs, bt->total, bt->smem_wy, bt->grid_wy, bt->grid_wz);
     if (rc) { free_batch(bt); return rc; }
   }
   c->batches[key] = bt;
@@ -522,21 +529,46 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   return 0;
 }
 
-// Shared memory and resident grid (in blocks of WF_WARPS warps, at most
-// one warp per unit) of the warp y transforms of a set of boxes.
-int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid) {
+// Shared memory and resident grids (in blocks of WF_WARPS warps, at most
+// one warp per unit) of the warp y and z transforms of a set of boxes.
+int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid, int *grid_z) {
   (void)devs;
+  int dev = 0, nsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   for (int c = 0; c < WY_NV; ++c) {
     smem[c] = wf_smem_bytes(WY_V[c]);
-    grid[c] = 0;
-    if (!total[FAM_WY8 + c]) continue;
-    int dev = 0, nsm = 0, occ = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    if (c == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, WF_T, smem[c]));
-    else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<12>, WF_T, smem[c]));
-    if (occ < 1) return fail(AFID_ESIZE, "warp transform block of %zu bytes does not fit an SM", smem[c]);
-    grid[c] = std::max(1, std::min((int)cdiv(total[FAM_WY8 + c], WF_WARPS), nsm * occ));
+    grid[c] = grid_z[c] = 0;
+    for (int zd = 0; zd < 2; ++zd) {
+      const int units = total[(zd ? FAM_WZ8 : FAM_WY8) + c];
+      if (!units) continue;
+      int occ = 0;
+      if (c == 0 && !zd) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, WF_T, smem[c]));
+      else if (!zd) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<12>, WF_T, smem[c]));
+      else if (c == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_z<-1, 8>, WF_T, smem[c]));
+      else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_z<-1, 12>, WF_T, smem[c]));
+      if (occ < 1) return fail(AFID_ESIZE, "warp transform block of %zu bytes does not fit an SM", smem[c]);
+      (zd ? grid_z : grid)[c] = std::max(1, std::min((int)cdiv(units, WF_WARPS), nsm * occ));
+    }
+  }
+  return 0;
+}
+
+// The z transforms of a batch (SGN -1 forward, +1 inverse): the tile kernel
+// for boxes without a warp plan, one warp-kernel launch per class present.
+template <int SGN, class BD>
+int launch_fft_z(const int *total, BD bd, int grid_z, size_t smem_z, FftSmem sm_z, const int *grid_wz,
+                 const size_t *smem_wy, cudaStream_t s, int ns) {
+  if (total[FAM_FZ] > 0) {
+    k_fft_z<SGN><<<grid_z, FFT_T, smem_z, s>>>(bd(FAM_FZ), ns, sm_z, total[FAM_FZ]);
+    CKL();
+  }
+  for (int c = 0; c < WY_NV; ++c) {
+    const int f = FAM_WZ8 + c;
+    if (!total[f]) continue;
+    if (c == 0) k_fftw_z<SGN, 8><<<grid_wz[c], WF_T, smem_wy[c], s>>>(bd(f), ns, total[f]);
+    else k_fftw_z<SGN, 12><<<grid_wz[c], WF_T, smem_wy[c], s>>>(bd(f), ns, total[f]);
+    CKL();
   }
   return 0;
 }
@@ -599,6 +631,10 @@ int init_kernel_attrs() {
   CK(cudaFuncSetAttribute(k_fftw_y_fwd<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fftw_y_inv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   CK(cudaFuncSetAttribute(k_fftw_y_inv<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_z<-1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_z<-1, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_z<+1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  CK(cudaFuncSetAttribute(k_fftw_z<+1, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
   done[dev] = true;
   return 0;
 }
@@ -651,16 +687,22 @@ int launch_poisson(const Batch *bt, cudaStream_t s, int ns, bool from_vel, Prof 
     if (rc) return rc;
   }
   PMARK(pf, AFID_K_FFT_Y_FWD);
-  k_fft_z<-1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
-  CKL();
+  {
+    int rc = launch_fft_z<-1>(bt->total, [&](int f) { return bdev(bt, f); }, bt->grid_z, bt->smem_z, bt->sm_z,
+                              bt->grid_wz, bt->smem_wy, s, ns);
+    if (rc) return rc;
+  }
   PMARK(pf, AFID_K_FFT_Z_FWD);
   {
     int rc = launch_poisson_x(bt->total, [&](int fam) { return bdev(bt, fam); }, s, ns);
     if (rc) return rc;
   }
   PMARK(pf, AFID_K_POISSON_X);
-  k_fft_z<+1><<<bt->grid_z, FFT_T, bt->smem_z, s>>>(bdev(bt, FAM_FZ), ns, bt->sm_z, bt->total[FAM_FZ]);
-  CKL();
+  {
+    int rc = launch_fft_z<+1>(bt->total, [&](int f) { return bdev(bt, f); }, bt->grid_z, bt->smem_z, bt->sm_z,
+                              bt->grid_wz, bt->smem_wy, s, ns);
+    if (rc) return rc;
+  }
   PMARK(pf, AFID_K_FFT_Z_INV);
   {
     int rc = launch_fft_y(false, bt->total, [&](int f) { return bdev(bt, f); }, bt->grid_y, bt->smem_y, bt->sm_y,
@@ -900,6 +942,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
     return fail(AFID_EFFT, "FFT size not efficient: nym=%d nzm=%d need prime factors <= 7 (code 444)", p->nym, p->nzm);
   }
   if (!warp_plan(d.nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np)) d.wy_v = 0;
+  if (!warp_plan(d.nzm, &d.wz_v, &d.wz_g, d.wz_rad, &d.wz_np)) d.wz_v = 0;
   Sizes s = sizes_of(*p);
   d.plane = s.plane; d.fsize = s.fsize; d.nspec = s.nspec;
   d.dx = (double)p->nxm / p->alx3; d.dy = (double)p->nym / p->ylen; d.dz = (double)p->nzm / p->zlen;
@@ -1231,6 +1274,9 @@ int afid_box_test_skip_z_copies(afid_ctx *c, int id, int skip, unsigned max_poll
   CK(cudaStreamSynchronize(c->stream));
   hb->dev.z_copy_skip = skip ? 1 : 0;
   hb->dev.mbar_tries = max_polls;
+  // the switch acts on the tile z kernel: a skipped box leaves the warp plan
+  BoxDev &d = hb->dev;
+  if (skip || !warp_plan(d.nzm, &d.wz_v, &d.wz_g, d.wz_rad, &d.wz_np)) d.wz_v = 0;
   // batches hold copies of the descriptor: drop the ones with this box
   for (auto it = c->batches.begin(); it != c->batches.end();) {
     bool has = false;
@@ -1822,6 +1868,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   if (factor_radices(nym, d.fft_y_radix, &d.fft_y_np) || factor_radices(nzm, d.fft_z_radix, &d.fft_z_np))
     return fail(AFID_EFFT, "noalloc: nym=%d nzm=%d need prime factors <= 7", nym, nzm);
   if (!warp_plan(nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np)) d.wy_v = 0;
+  if (!warp_plan(nzm, &d.wz_v, &d.wz_g, d.wz_rad, &d.wz_np)) d.wz_v = 0;
   int dev = 0;
   CK(cudaGetDevice(&dev));
   int rc = noalloc_setup(dev);
@@ -1925,22 +1972,22 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   const size_t sy = (size_t)(2 * smy.slot + twy) * 16 + FFT_TAIL_BYTES;
   const size_t sz = (size_t)(2 * smz.slot + twz) * 16 + FFT_TAIL_BYTES;
   size_t swy[WY_NV];
-  int gwy[WY_NV];
+  int gwy[WY_NV], gwz[WY_NV];
   rc = fft_grid(k_fft_y_fwd, sy, total[FAM_FY], &gy);
   if (!rc) rc = fft_grid(k_fft_z<-1>, sz, total[FAM_FZ], &gz);
-  if (!rc) rc = wy_shapes(std::vector<BoxDev>{d}, total, swy, gwy);
+  if (!rc) rc = wy_shapes(std::vector<BoxDev>{d}, total, swy, gwy, gwz);
   if (rc) return rc;
   // the x-solve's pivots, for this call's grid
   k_poisson_pivots<<<(unsigned)cdiv(px_pairs(nzm, d.nymh), 256), 256, 0, st>>>(d);
   CKL();
   rc = launch_fft_y(true, total, bd, gy, sy, smy, gwy, swy, st, 0);
   if (rc) return rc;
-  k_fft_z<-1><<<gz, FFT_T, sz, st>>>(bd(FAM_FZ), 0, smz, total[FAM_FZ]);
-  CKL();
+  rc = launch_fft_z<-1>(total, bd, gz, sz, smz, gwz, swy, st, 0);
+  if (rc) return rc;
   rc = launch_poisson_x(total, bd, st, 0);
   if (rc) return rc;
-  k_fft_z<+1><<<gz, FFT_T, sz, st>>>(bd(FAM_FZ), 0, smz, total[FAM_FZ]);
-  CKL();
+  rc = launch_fft_z<+1>(total, bd, gz, sz, smz, gwz, swy, st, 0);
+  if (rc) return rc;
   rc = launch_fft_y(false, total, bd, gy, sy, smy, gwy, swy, st, 0);
   if (rc) return rc;
   if (status) {

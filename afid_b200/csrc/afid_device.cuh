@@ -115,6 +115,9 @@ struct BoxDev {
   // lane (0: no plan, the tile kernels run), wy_g lanes per line, radices
   int wy_v, wy_g, wy_np;
   int wy_rad[8];
+  // the same for the z transforms (k_fftw_z): 0 = the tile kernel runs
+  int wz_v, wz_g, wz_np;
+  int wz_rad[8];
   // test switch of the bounded waits (afid_box_test_skip_z_copies): the z
   // transform arms its slot mbarriers without issuing the box's tile copies,
   // and its waits give up after mbar_tries polls (0: MBAR_MAX_TRIES)

@@ -1,5 +1,6 @@
 // Warp transforms along y (the r2c and c2r steps of
-// SolvePressureCorrection.F90:97 and :148).
+// SolvePressureCorrection.F90:97 and :148) and along z (the c2c steps of
+// SolvePressureCorrection.F90:102 and :141).
 //
 // Each warp transforms LPW = 32 / G complex lines of length N on its own:
 // G lanes per line, V = N / G values per lane (8 or 12).  The plan is a mixed-radix
@@ -34,6 +35,11 @@ __host__ __device__ __forceinline__ int wy_lpw(const BoxDev &B) { return 32 / B.
 __host__ __device__ __forceinline__ int wy_units_per_plane(const BoxDev &B) {
   return (B.nzm + 2 * wy_lpw(B) - 1) / (2 * wy_lpw(B));
 }
+// the same for the z plan: a unit is LPW neighbouring ky columns of a plane
+__host__ __device__ __forceinline__ int wz_lpw(const BoxDev &B) { return 32 / B.wz_g; }
+__host__ __device__ __forceinline__ int wz_units_per_plane(const BoxDev &B) {
+  return (B.nymh + wz_lpw(B) - 1) / wz_lpw(B);
+}
 
 // a warp's slice of shared memory: twiddles (WF_MAX_N complex), radices
 // (8 ints, 32 bytes), then the work region (32 V complex)
@@ -55,7 +61,9 @@ struct WarpUnits {
 };
 
 // The fields of a box a warp transform needs, held in registers; load()
-// also copies the box's twiddles and radices into the warp's slice.
+// also copies the box's twiddles and radices into the warp's slice.  ZDIR
+// selects the z plan: lines of nzm points, LPW columns per unit.
+template <bool ZDIR = false>
 struct WarpBox {
   int b, N, nzm, nh, nxm, lpw, lgL, upp, np;
   long long plane;
@@ -65,23 +73,23 @@ struct WarpBox {
   __device__ __forceinline__ void load(const BatchDev &bt, int bi, int ns, double2 *tws, int *rad) {
     const BoxDev *Bp = bt.boxes + bi;
     b = bi;
-    N = __ldg(&Bp->nym);
     nzm = __ldg(&Bp->nzm);
     nh = __ldg(&Bp->nymh);
     nxm = __ldg(&Bp->nxm);
-    lpw = 32 / __ldg(&Bp->wy_g);
+    N = ZDIR ? nzm : __ldg(&Bp->nym);
+    lpw = 32 / __ldg(ZDIR ? &Bp->wz_g : &Bp->wy_g);
     lgL = ilog2(lpw);
-    upp = (nzm + 2 * lpw - 1) / (2 * lpw);
-    np = __ldg(&Bp->wy_np);
+    upp = ZDIR ? (nh + lpw - 1) / lpw : (nzm + 2 * lpw - 1) / (2 * lpw);
+    np = __ldg(ZDIR ? &Bp->wz_np : &Bp->wy_np);
     plane = __ldg(&Bp->plane);
     phi = (double *)__ldg((const unsigned long long *)&Bp->phi);
     spec = (double2 *)__ldg((const unsigned long long *)&Bp->spec);
-    const double2 *twy = (const double2 *)__ldg((const unsigned long long *)&Bp->twy);
+    const double2 *tw = (const double2 *)__ldg((const unsigned long long *)(ZDIR ? &Bp->twz : &Bp->twy));
     run = __ldg(&Bp->active) && ns < __ldg(&Bp->nsst) &&
           *(volatile int *)&((BoxScalars *)__ldg((const unsigned long long *)&Bp->sc))->status == 0;
     const int lane = threadIdx.x & 31;
-    for (int q = lane; q < N; q += 32) tws[q] = __ldg(twy + q);
-    if (lane < 8) rad[lane] = __ldg(&Bp->wy_rad[lane]);
+    for (int q = lane; q < N; q += 32) tws[q] = __ldg(tw + q);
+    if (lane < 8) rad[lane] = __ldg(ZDIR ? &Bp->wz_rad[lane] : &Bp->wy_rad[lane]);
     __syncwarp();
   }
 };
@@ -174,7 +182,7 @@ __global__ void __launch_bounds__(WF_T, 2) k_fftw_y_fwd(BatchDev bt, int ns, int
   const WarpUnits wu(total);
   if (wu.first() >= total) return;
   TileWalk wk(bt, wu.first());
-  WarpBox X;
+  WarpBox<> X;
   X.b = -1;
   for (int u = wu.first(); u < total; u = wu.next(u)) {
     const int lu = wk.to(bt, u);
@@ -243,7 +251,7 @@ __global__ void __launch_bounds__(WF_T, 2) k_fftw_y_inv(BatchDev bt, int ns, int
   const WarpUnits wu(total);
   if (wu.first() >= total) return;
   TileWalk wk(bt, wu.first());
-  WarpBox X;
+  WarpBox<> X;
   X.b = -1;
   for (int u = wu.first(); u < total; u = wu.next(u)) {
     const int lu = wk.to(bt, u);
@@ -255,6 +263,51 @@ __global__ void __launch_bounds__(WF_T, 2) k_fftw_y_inv(BatchDev bt, int ns, int
     const double2 *half = X.spec + (long long)k * X.nzm * nh + (long long)i0 * nh;
     double *rows = X.phi + (long long)k * X.plane + (long long)i0 * N;
     wfft<+1, V>(reg, N, lgL, rad, X.np, tws, WHalfPairSrc{half, N, nh, nrow}, WRowPairDst{rows, N, nrow});
+  }
+}
+
+// z lines: column ky0 + l of one plane's spectrum (row pitch nh), read and
+// written in place in HBM; columns at or beyond nh read as zero and are not
+// stored.  Every value a warp's pass reads is read before any is written
+// (wpass loads all its inputs ahead of a __syncwarp), so a single-pass plan
+// is in place too.
+struct WColSrc {
+  const double2 *S;
+  int nh, ky0;
+  __device__ __forceinline__ double2 operator()(int l, int n) const {
+    return ky0 + l < nh ? __ldcg(S + (long long)n * nh + ky0 + l) : make_double2(0.0, 0.0);
+  }
+};
+struct WColDst {
+  double2 *S;
+  int nh, ky0;
+  __device__ __forceinline__ void operator()(int l, int n, double2 v) const {
+    if (ky0 + l < nh) __stcg(S + (long long)n * nh + ky0 + l, v);
+  }
+};
+
+// c2c z transform (SGN -1 forward, +1 inverse) of the units of the launch:
+// a unit is LPW neighbouring ky columns of one plane, so the lanes reading
+// one kz row of the unit read LPW consecutive complex values, and the runs of
+// units that neighbouring warps take cover neighbouring columns of the rows.
+template <int SGN, int V>
+__global__ void __launch_bounds__(WF_T, 2) k_fftw_z(BatchDev bt, int ns, int total) {
+  extern __shared__ double2 wsm[];
+  double2 *const tws = wsm + (threadIdx.x >> 5) * wf_slice(V);
+  int *const rad = reinterpret_cast<int *>(tws + WF_MAX_N);
+  double2 *const reg = tws + WF_MAX_N + 2;
+  const WarpUnits wu(total);
+  if (wu.first() >= total) return;
+  TileWalk wk(bt, wu.first());
+  WarpBox<true> X;
+  X.b = -1;
+  for (int u = wu.first(); u < total; u = wu.next(u)) {
+    const int lu = wk.to(bt, u);
+    if (wk.b != X.b) X.load(bt, wk.b, ns, tws, rad);
+    if (!X.run) continue;
+    const int k = lu / X.upp, ky0 = (lu - k * X.upp) * X.lpw;
+    double2 *const S = X.spec + (long long)k * X.nzm * X.nh;
+    wfft<SGN, V>(reg, X.N, X.lgL, rad, X.np, tws, WColSrc{S, X.nh, ky0}, WColDst{S, X.nh, ky0});
   }
 }
 
