@@ -114,13 +114,15 @@ int factor_radices(int n, int *rad, int *np) {
 
 // Warp plan of an n-point transform (k_fftw.cuh): V values per lane (8 or
 // 12; 16 and 24 spilled registers at two blocks per SM), G = n / V lanes per
-// line (a power of two <= 32), and a radix sequence whose radices all divide
-// V, power-of-two radices first; the fewest passes win, then the fewer
-// values per lane.  Returns 0 (no plan) for sizes the tile kernels keep:
-// lines longer than WARP_PLAN_MAX_N, where the tile kernels measured faster
-// (384 and 768 points).
+// line (a power of two, min_g <= G <= 32), and a radix sequence whose
+// radices all divide V, power-of-two radices first; the fewest passes win,
+// then the fewer values per lane.  The y transforms need min_g = 2: their
+// staged rows (2 LPW rows of N + 2 doubles, or of N/2 + 1 complex values)
+// fit a warp buffer only with LPW = 32 / G <= 16.  Returns 0 (no plan) for
+// sizes the tile kernels keep: lines longer than WARP_PLAN_MAX_N, where the
+// tile kernels measured faster (384 and 768 points).
 constexpr int WARP_PLAN_MAX_N = WF_MAX_N;
-int warp_plan(int n, int *v_out, int *g_out, int *rad, int *np) {
+int warp_plan(int n, int *v_out, int *g_out, int *rad, int *np, int min_g = 1) {
   static const int cand[7] = {16, 12, 8, 6, 4, 3, 2};
   if (n > WARP_PLAN_MAX_N) return 0;
   int best_v = 0, best_np = 99, best[8] = {};
@@ -128,7 +130,7 @@ int warp_plan(int n, int *v_out, int *g_out, int *rad, int *np) {
     const int V = WY_V[vi];
     if (n % V) continue;
     const int G = n / V;
-    if (G > 32 || (G & (G - 1))) continue;
+    if (G < min_g || G > 32 || (G & (G - 1))) continue;
     // depth-first search for the shortest factorisation into radices dividing V
     int cur[8], found[8] = {}, found_np = 99;
     std::function<void(int, int)> dfs = [&](int m, int d) {
@@ -529,8 +531,8 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
   return 0;
 }
 
-// Shared memory and resident grids (in blocks of WF_WARPS warps, at most
-// one warp per unit) of the warp y and z transforms of a set of boxes.
+// Shared memory and resident grids (in blocks of wf_warps(V) warps, at
+// most one warp per unit) of the warp y and z transforms of a set of boxes.
 int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, int *grid, int *grid_z) {
   (void)devs;
   int dev = 0, nsm = 0;
@@ -543,12 +545,13 @@ int wy_shapes(const std::vector<BoxDev> &devs, const int *total, size_t *smem, i
       const int units = total[(zd ? FAM_WZ8 : FAM_WY8) + c];
       if (!units) continue;
       int occ = 0;
-      if (c == 0 && !zd) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, WF_T, smem[c]));
-      else if (!zd) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<12>, WF_T, smem[c]));
-      else if (c == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_z<-1, 8>, WF_T, smem[c]));
-      else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_z<-1, 12>, WF_T, smem[c]));
+      const int nt = 32 * wf_warps(WY_V[c]);
+      if (c == 0 && !zd) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<8>, nt, smem[c]));
+      else if (!zd) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_y_fwd<12>, nt, smem[c]));
+      else if (c == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_z<-1, 8>, nt, smem[c]));
+      else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fftw_z<-1, 12>, nt, smem[c]));
       if (occ < 1) return fail(AFID_ESIZE, "warp transform block of %zu bytes does not fit an SM", smem[c]);
-      (zd ? grid_z : grid)[c] = std::max(1, std::min((int)cdiv(units, WF_WARPS), nsm * occ));
+      (zd ? grid_z : grid)[c] = std::max(1, std::min((int)cdiv(units, wf_warps(WY_V[c])), nsm * occ));
     }
   }
   return 0;
@@ -566,8 +569,8 @@ int launch_fft_z(const int *total, BD bd, int grid_z, size_t smem_z, FftSmem sm_
   for (int c = 0; c < WY_NV; ++c) {
     const int f = FAM_WZ8 + c;
     if (!total[f]) continue;
-    if (c == 0) k_fftw_z<SGN, 8><<<grid_wz[c], WF_T, smem_wy[c], s>>>(bd(f), ns, total[f]);
-    else k_fftw_z<SGN, 12><<<grid_wz[c], WF_T, smem_wy[c], s>>>(bd(f), ns, total[f]);
+    if (c == 0) k_fftw_z<SGN, 8><<<grid_wz[c], 32 * wf_warps(8), smem_wy[c], s>>>(bd(f), ns, total[f]);
+    else k_fftw_z<SGN, 12><<<grid_wz[c], 32 * wf_warps(12), smem_wy[c], s>>>(bd(f), ns, total[f]);
     CKL();
   }
   return 0;
@@ -588,11 +591,11 @@ int launch_fft_y(bool fwd, const int *total, BD bd, int grid_y, size_t smem_y, F
     if (!total[f]) continue;
     const BatchDev b = bd(f);
     if (c == 0) {
-      if (fwd) k_fftw_y_fwd<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
-      else k_fftw_y_inv<8><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+      if (fwd) k_fftw_y_fwd<8><<<grid_wy[c], 32 * wf_warps(8), smem_wy[c], s>>>(b, ns, total[f]);
+      else k_fftw_y_inv<8><<<grid_wy[c], 32 * wf_warps(8), smem_wy[c], s>>>(b, ns, total[f]);
     } else {
-      if (fwd) k_fftw_y_fwd<12><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
-      else k_fftw_y_inv<12><<<grid_wy[c], WF_T, smem_wy[c], s>>>(b, ns, total[f]);
+      if (fwd) k_fftw_y_fwd<12><<<grid_wy[c], 32 * wf_warps(12), smem_wy[c], s>>>(b, ns, total[f]);
+      else k_fftw_y_inv<12><<<grid_wy[c], 32 * wf_warps(12), smem_wy[c], s>>>(b, ns, total[f]);
     }
     CKL();
   }
@@ -941,7 +944,7 @@ int afid_box_add(afid_ctx *c, const afid_box_params *p, const double *xc, int *b
     delete hb;
     return fail(AFID_EFFT, "FFT size not efficient: nym=%d nzm=%d need prime factors <= 7 (code 444)", p->nym, p->nzm);
   }
-  if (!warp_plan(d.nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np)) d.wy_v = 0;
+  if (!warp_plan(d.nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np, 2)) d.wy_v = 0;
   if (!warp_plan(d.nzm, &d.wz_v, &d.wz_g, d.wz_rad, &d.wz_np)) d.wz_v = 0;
   Sizes s = sizes_of(*p);
   d.plane = s.plane; d.fsize = s.fsize; d.nspec = s.nspec;
@@ -1867,7 +1870,7 @@ extern "C" int afid_solve_pressure_correction_noalloc(double *dph, int nxm, int 
   memset(&d, 0, sizeof d);
   if (factor_radices(nym, d.fft_y_radix, &d.fft_y_np) || factor_radices(nzm, d.fft_z_radix, &d.fft_z_np))
     return fail(AFID_EFFT, "noalloc: nym=%d nzm=%d need prime factors <= 7", nym, nzm);
-  if (!warp_plan(nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np)) d.wy_v = 0;
+  if (!warp_plan(nym, &d.wy_v, &d.wy_g, d.wy_rad, &d.wy_np, 2)) d.wy_v = 0;
   if (!warp_plan(nzm, &d.wz_v, &d.wz_g, d.wz_rad, &d.wz_np)) d.wz_v = 0;
   int dev = 0;
   CK(cudaGetDevice(&dev));
