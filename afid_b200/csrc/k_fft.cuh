@@ -362,19 +362,26 @@ struct FftSmem {
   int tw;     // complex values of the twiddle table (the z transform's mbarriers follow it)
 };
 
-// A persistent block takes runs of FFT_TILE_RUN consecutive tiles, the runs
-// dealt round-robin over the blocks (block p: runs p, p + G, p + 2G, ...):
+// A persistent block takes runs of consecutive tiles, the runs dealt
+// round-robin over the blocks (block p: runs p, p + G, p + 2G, ...):
 // neighbouring blocks work on neighbouring tiles at the same time, the work
 // of boxes of different sizes spreads over all blocks, and a block changes
-// boxes at most once per run.  A walker follows the tiles' boxes forward.
+// boxes at most once per run.  Runs are FFT_TILE_RUN long when every worker
+// of the grid (block, or warp of the warp transforms) gets at least that many
+// items, else 2 or 1 long, so that a small launch spreads over all workers.
+// A walker follows the tiles' boxes forward.
 constexpr int FFT_TILE_RUN = 4;
+__device__ __forceinline__ int run_log2(int total, int workers) {
+  return total >= FFT_TILE_RUN * workers ? 2 : total >= 2 * workers ? 1 : 0;
+}
 struct TileRange {
-  int t0, total;
-  __device__ __forceinline__ explicit TileRange(int total_) : t0(blockIdx.x * FFT_TILE_RUN), total(total_) {}
+  int t0, total, lgr;
+  __device__ __forceinline__ explicit TileRange(int total_)
+      : total(total_), lgr(run_log2(total_, (int)gridDim.x)) { t0 = (int)blockIdx.x << lgr; }
   __device__ __forceinline__ int first() const { return t0 < total ? t0 : total; }
   __device__ __forceinline__ int next(int t) const {
     int n = t + 1;
-    if (n % FFT_TILE_RUN == 0) n = (t / FFT_TILE_RUN + (int)gridDim.x) * FFT_TILE_RUN;
+    if ((n & ((1 << lgr) - 1)) == 0) n = ((t >> lgr) + (int)gridDim.x) << lgr;
     return n < total ? n : total;
   }
 };

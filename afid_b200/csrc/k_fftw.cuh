@@ -13,8 +13,8 @@
 // Warps are independent: a warp unit is LPW lines of one plane of one box
 // (2 LPW rows for y, LPW neighbouring ky columns for z), the units of a
 // launch are numbered across its boxes, and each warp of the (persistent)
-// grid takes runs of WF_RUN consecutive units, the runs dealt round-robin
-// over all warps.  A warp keeps the fields of its current box in registers
+// grid takes runs of consecutive units (4, or 2 or 1 in a launch with
+// fewer than 4 units per warp), the runs dealt round-robin over all warps.  A warp keeps the fields of its current box in registers
 // and that box's twiddles and radices in its slice, reloading them (with
 // __syncwarp only) when its unit belongs to another box: a block has no
 // barrier at all.
@@ -29,7 +29,6 @@
 
 namespace afid {
 
-constexpr int WF_RUN = 4;              // consecutive units per run of a warp
 constexpr int WF_MAX_N = 128;          // longest line with a warp plan
 
 // lines per warp and units per plane of box B's y plan
@@ -57,18 +56,19 @@ __host__ __device__ constexpr int wf_buf(int V) { return 32 * V + 32; }
 __host__ __device__ constexpr int wf_slice(int V) { return WF_MAX_N + 2 + 2 * wf_buf(V); }
 __host__ __device__ constexpr size_t wf_smem_bytes(int V) { return (size_t)wf_warps(V) * wf_slice(V) * 16; }
 
-// The unit sequence of a warp: runs gw, gw + NW, gw + 2 NW, ... of WF_RUN
-// units (gw: the warp's index in the grid of W-warp blocks, NW: the grid's
-// warps).
+// The unit sequence of a warp: runs gw, gw + NW, gw + 2 NW, ... of units
+// (gw: the warp's index in the grid of W-warp blocks, NW: the grid's warps;
+// run lengths as for the tile kernels' TileRange).
 template <int W>
 struct WarpUnits {
-  int gw, nw, total;
+  int gw, nw, total, lgr;
   __device__ __forceinline__ explicit WarpUnits(int total_)
-      : gw((int)(blockIdx.x * W + (threadIdx.x >> 5))), nw((int)(gridDim.x * W)), total(total_) {}
-  __device__ __forceinline__ int first() const { return gw * WF_RUN < total ? gw * WF_RUN : total; }
+      : gw((int)(blockIdx.x * W + (threadIdx.x >> 5))), nw((int)(gridDim.x * W)), total(total_),
+        lgr(run_log2(total_, (int)(gridDim.x * W))) {}
+  __device__ __forceinline__ int first() const { return (gw << lgr) < total ? (gw << lgr) : total; }
   __device__ __forceinline__ int next(int u) const {
     int n = u + 1;
-    if (n % WF_RUN == 0) n = (u / WF_RUN + nw) * WF_RUN;
+    if ((n & ((1 << lgr) - 1)) == 0) n = ((u >> lgr) + nw) << lgr;
     return n < total ? n : total;
   }
 };

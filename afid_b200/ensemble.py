@@ -129,3 +129,34 @@ def compare(ctx, cfgs, nsteps: int, warmup: int = 2, seed0: int = 0) -> dict:
             "plain_mpoint_steps_s": ncell * nsteps / t_p / 1e6,
             "speedup": t_p / t_b, "status": st_b,
             "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+
+
+def main(argv=None) -> int:
+    """``python -m afid_b200.ensemble``: advance the seeded ensemble on one
+    GPU and print its device time per step (a small driver for profiling
+    the batched step outside the benchmark)."""
+    import argparse
+    import json
+
+    from .solver import Context
+    ap = argparse.ArgumentParser(prog="python -m afid_b200.ensemble")
+    ap.add_argument("--boxes", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--graph", action="store_true", help="step through the per-step CUDA graph")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    cfgs = ensemble_configs(a.boxes, seed=a.seed)
+    with Context(a.device) as ctx:
+        boxes = make_boxes(ctx, cfgs)
+        t = run_batched(ctx, boxes, a.steps, graph=a.graph)
+        status = [b.scalars()["status"] for b in boxes]
+        print(json.dumps({"boxes": len(cfgs), "cells": sum(cells(c) for c in cfgs), "steps": a.steps,
+                          "ms_per_step": t / a.steps * 1e3, "status_ok": all(s == 0 for s in status)}))
+        for b in boxes:
+            ctx.remove_box(b)
+    return 0 if all(s == 0 for s in status) else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

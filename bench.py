@@ -142,18 +142,66 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled from a thread every 5 ms (the region can be shorter
+    than nvidia-smi's start-up), nvidia-smi as the fallback.  Only samples
+    taken between start() and stop() count; start() returns once the first
+    sample is in."""
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.lines: list[str] = []
         self.th = None
+        self.nv = None
+        self.samples: list[tuple[float, float, int]] = []
+        self.smax = None
+        self.run = False
+        self.t0 = self.t1 = 0.0
+
+    def _nvml_handle(self):
+        import pynvml as N
+        import torch
+        N.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        try:
+            return N, N.nvmlDeviceGetHandleByPciBusId(
+                f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll(self, N, h):
+        while self.run:
+            try:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                rs = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.monotonic(), float(sm), int(rs)))
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def start(self):
+        try:
+            N, h = self._nvml_handle()
+            self.smax = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            self.nv = (N, {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+                           "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+                           "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+                           "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap})
+            self.run = True
+            self.th = threading.Thread(target=self._poll, args=(N, h), daemon=True)
+            self.th.start()
+            t_end = time.monotonic() + 1.0
+            while not self.samples and time.monotonic() < t_end:
+                time.sleep(0.001)
+            self.t0 = time.monotonic()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
@@ -169,8 +217,21 @@ class ClockSampler:
             self.lines.append(ln.strip())
 
     def stop(self) -> dict:
+        if self.nv is not None:
+            self.t1 = time.monotonic()
+            time.sleep(0.006)
+            self.run = False
+            self.th.join(timeout=2)
+            N, bits = self.nv
+            inside = [(sm, rs) for t, sm, rs in self.samples if self.t0 <= t <= self.t1]
+            if not inside and self.samples:   # a region shorter than one poll: the nearest sample
+                inside = [min(((abs(t - self.t0), sm, rs) for t, sm, rs in self.samples))[1:]]
+            reasons = sorted({nm for _, rs in inside for nm, bit in bits.items() if rs & bit})
+            return {"sm_mhz": statistics.median([sm for sm, _ in inside]) if inside else None,
+                    "sm_max_mhz": self.smax, "reasons": reasons, "samples": len(inside),
+                    "source": "NVML, 5 ms polling during the timed region"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -179,7 +240,6 @@ class ClockSampler:
         if self.th:
             self.th.join(timeout=2)
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 7:
@@ -189,11 +249,11 @@ class ClockSampler:
                 smax = float(parts[1])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[3:7]):
+            for nm, v in zip(self.NAMES, parts[3:7]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi -lms 100"}
 
 
 def dist_env():
