@@ -71,6 +71,9 @@ NCU_TRAFFIC_BYTES_PER_CELL: dict[str, float] = {
     "explicit_fwd": 135.5, "implicit_bwd": 94.9, "divergence": 31.4, "fft_y_fwd": 14.3,
     "fft_z_fwd": 14.3, "poisson_x": 30.3, "fft_z_inv": 14.4, "fft_y_inv": 14.5, "diag": 32.4,
 }
+# the same from an ncu capture of the 64-box ensemble itself
+# (python -m afid_b200.ensemble --steps 2, fourth explicit-kernel launch)
+NCU_TRAFFIC_BYTES_PER_CELL_ENSEMBLE: dict[str, float] = {"explicit_fwd": 134.9}
 
 
 # ----------------------------------------------------------------------------
@@ -423,7 +426,7 @@ def timed_steps(ctx, stream, boxes, nsteps, D: Dist, fn=None):
     return D.max(e0.elapsed_time(e1))
 
 
-def roofline_of(ctx, boxes, cfgs, prof_steps=2):
+def roofline_of(ctx, boxes, cfgs, prof_steps=2, ensemble=False):
     prof = ctx.step_profiled(boxes, prof_steps)
     launches_per_step = sum(c for _, c in prof.values()) / prof_steps
     ncell = sum(cells(c) for c in cfgs)
@@ -436,7 +439,8 @@ def roofline_of(ctx, boxes, cfgs, prof_steps=2):
     avg_s = top_ms / 1e3 / prof[top][1]
     peak, peak_kind = load_peaks()
     achieved = kb[top] / avg_s / 1e9
-    traffic = NCU_TRAFFIC_BYTES_PER_CELL[top] * ncell if top in NCU_TRAFFIC_BYTES_PER_CELL else None
+    table = NCU_TRAFFIC_BYTES_PER_CELL_ENSEMBLE if ensemble else NCU_TRAFFIC_BYTES_PER_CELL
+    traffic = table[top] * ncell if top in table else None
     per_kernel = {}
     for k, (t_ms, c) in prof.items():
         if c == 0:
@@ -448,7 +452,8 @@ def roofline_of(ctx, boxes, cfgs, prof_steps=2):
     return {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": f"{peak_kind} copy bandwidth (of measured)",
             "bytes_per_launch": kb[top], "avg_launch_ms": avg_s * 1e3, "traffic": traffic,
-            "traffic_source": "ncu dram bytes per cell of a 193x384x384 capture, times the cells",
+            "traffic_source": ("ncu dram bytes per cell of a capture of the same 64 boxes, times the cells"
+                               if ensemble else "ncu dram bytes per cell of a 193x384x384 capture, times the cells"),
             "kernel_ms_per_step": {k: v["ms_per_step"] for k, v in per_kernel.items()},
             "per_kernel": per_kernel}, launches_per_step
 
@@ -596,11 +601,11 @@ def gpu_arm(args):
     statuses = [b.scalars()["status"] for b in boxes]
     div_max = max(max(h["divmax"] for h in b.history(args.steps)) for b in boxes)
 
-    roof, launches_per_step = roofline_of(ctx, boxes, cfgs)
+    roof, launches_per_step = roofline_of(ctx, boxes, cfgs, ensemble=(args.workload == "batch"))
     e2e = e2e_run(ctx, boxes, cfgs, seeds, args.steps, D)
 
     batched = None
-    if args.workload == "batch":
+    if args.workload == "batch" and not args.no_plain:
         if not args.no_tune:                 # each box alone runs its own class's best shapes
             per_class = autotune.tune(ctx, cfgs)
             for b in boxes:
@@ -709,6 +714,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="use the built-in launch shapes")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream sub-record")
     ap.add_argument("--no-c2", action="store_true", help="skip the large-box sub-record")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the one-box-at-a-time comparison of the batch workload")
     ap.add_argument("--rate", type=float, default=50.0, help="arrivals/s of the serve sub-record")
     ap.add_argument("--serve", action="store_true", help="run the served-stream sweep over --rates")
     ap.add_argument("--rates", type=float, nargs="+", default=[1.0, 10.0, 50.0, 200.0])

@@ -128,3 +128,20 @@ def test_pressure_solve_x_sizes(ctx, nxm):
     O.solve_pressure_correction(s)
     assert rel_l2(box.download("dph"), s.dph, remove_mean=True) <= 1e-11
     ctx.remove_box(box)
+
+
+@pytest.mark.parametrize("nym,nzm", [(8, 12), (12, 8), (16, 24), (8, 8), (24, 16)])
+def test_pressure_solve_short_lines(ctx, nym, nzm):
+    """SolvePressureCorrection on the shortest transform lines: 8 and
+    12 points are one warp lane per line in the z transform (32 lines per
+    warp) and leave the y transform to the tile kernel (its staged rows need
+    at least two lanes per line); 16 and 24 points are two lanes per line."""
+    cfg = cfg_of(20, nym, nzm, ray=1e6, ylen=1.3, zlen=0.9)
+    s = oracle_state(cfg, seed=None)
+    s.dph[...] = np.random.default_rng(nym * 100 + nzm).standard_normal(s.dph.shape)
+    box = ctx.add_box(cfg, s.g.xc)
+    box.upload("dph", s.dph)
+    box.solve_pressure_correction()
+    O.solve_pressure_correction(s)
+    assert rel_l2(box.download("dph"), s.dph, remove_mean=True) <= 1e-12
+    ctx.remove_box(box)
