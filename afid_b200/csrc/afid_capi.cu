@@ -381,6 +381,9 @@ struct afid_ctx {
   int next_id = 0;
   std::map<std::vector<int>, Batch *> batches;
   std::vector<double> staging_host;
+  // staging of afid_boxes_get_scalars: device and pinned host records
+  BoxScalars *d_sc_stage = nullptr, *h_sc_stage = nullptr;
+  int sc_stage_n = 0;
 };
 
 namespace {
@@ -855,6 +858,8 @@ int afid_ctx_destroy(afid_ctx *c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (auto &kv : c->batches) free_batch(kv.second);
+  if (c->d_sc_stage) cudaFree(c->d_sc_stage);
+  if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
   for (auto &kv : c->boxes) {
     HostBox *hb = kv.second;
     cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small);
@@ -1056,7 +1061,7 @@ int afid_box_remove(afid_ctx *c, int id) {
   return 0;
 }
 
-static int transfer(afid_ctx *c, int id, int field, double *host, bool up) {
+static int transfer(afid_ctx *c, int id, int field, double *host, bool up, bool sync = true) {
   if (!c || !host) return fail(AFID_EINVAL, "null argument");
   HostBox *hb;
   int rc = get_box(c, id, &hb);
@@ -1077,7 +1082,7 @@ static int transfer(afid_ctx *c, int id, int field, double *host, bool up) {
     const size_t bytes = (size_t)d.plane * sizeof(double);
     if (up) CK(cudaMemcpyAsync(dp, host, bytes, cudaMemcpyHostToDevice, st));
     else CK(cudaMemcpyAsync(host, dp, bytes, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    if (sync) CK(cudaStreamSynchronize(st));
     return 0;
   }
   const size_t n = (size_t)rows * d.plane;
@@ -1096,7 +1101,7 @@ static int transfer(afid_ctx *c, int id, int field, double *host, bool up) {
     CKL();
     CK(cudaMemcpyAsync(host, stg, n * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
-  CK(cudaStreamSynchronize(st));
+  if (sync) CK(cudaStreamSynchronize(st));
   return 0;
 }
 
@@ -1106,6 +1111,17 @@ int afid_box_upload(afid_ctx *c, int id, int field, const double *host) {
 
 int afid_box_download(afid_ctx *c, int id, int field, double *host) {
   return transfer(c, id, field, host, false);
+}
+
+// The same copies queued on the context's stream without waiting: the
+// box's staging buffer is reused by the next transfer of the same box in
+// stream order, so queued transfers of one box do not overwrite each other.
+int afid_box_upload_async(afid_ctx *c, int id, int field, const double *host) {
+  return transfer(c, id, field, const_cast<double *>(host), true, false);
+}
+
+int afid_box_download_async(afid_ctx *c, int id, int field, double *host) {
+  return transfer(c, id, field, host, false, false);
 }
 
 int afid_box_reset(afid_ctx *c, int id, double dt) {
@@ -1232,6 +1248,44 @@ int afid_box_interp_field(afid_ctx *c, int id, int field, const double *old, int
   return 0;
 }
 
+static void scalars_out(const BoxScalars &bs, afid_box_scalars *out) {
+  out->dt = bs.dt; out->time = bs.time; out->cfl = bs.cfl; out->cfl_used = bs.cfl_used;
+  out->divmax = bs.divmax;
+  for (int q = 0; q < 3; ++q) out->vmax[q] = bs.vmax[q];
+  out->nu_bot = bs.nu_bot; out->nu_top = bs.nu_top; out->ntime = bs.ntime; out->status = bs.status;
+}
+
+__global__ void k_gather_scalars(const BoxDev *boxes, int n, BoxScalars *dst) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) dst[b] = *boxes[b].sc;
+}
+
+int afid_boxes_get_scalars(afid_ctx *c, const int *ids, int n, afid_box_scalars *out) {
+  if (!c || !ids || !out || n <= 0) return fail(AFID_EINVAL, "boxes_get_scalars: null argument or n <= 0");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  if (n > c->sc_stage_n) {
+    if (c->d_sc_stage) cudaFree(c->d_sc_stage);
+    if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
+    c->d_sc_stage = nullptr;
+    c->h_sc_stage = nullptr;
+    c->sc_stage_n = 0;
+    if (cudaMalloc(&c->d_sc_stage, sizeof(BoxScalars) * n) != cudaSuccess ||
+        cudaMallocHost(&c->h_sc_stage, sizeof(BoxScalars) * n) != cudaSuccess)
+      return fail(AFID_ENOMEM, "boxes_get_scalars: staging of %d records", n);
+    c->sc_stage_n = n;
+  }
+  k_gather_scalars<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, c->d_sc_stage);
+  CKL();
+  CK(cudaMemcpyAsync(c->h_sc_stage, c->d_sc_stage, sizeof(BoxScalars) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int b = 0; b < n; ++b) scalars_out(c->h_sc_stage[b], out + b);
+  return 0;
+}
+
 int afid_box_get_scalars(afid_ctx *c, int id, afid_box_scalars *out) {
   if (!c || !out) return fail(AFID_EINVAL, "null argument");
   HostBox *hb;
@@ -1242,10 +1296,7 @@ int afid_box_get_scalars(afid_ctx *c, int id, afid_box_scalars *out) {
   BoxScalars bs;
   CK(cudaMemcpyAsync(&bs, hb->dev.sc, sizeof bs, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  out->dt = bs.dt; out->time = bs.time; out->cfl = bs.cfl; out->cfl_used = bs.cfl_used;
-  out->divmax = bs.divmax;
-  for (int q = 0; q < 3; ++q) out->vmax[q] = bs.vmax[q];
-  out->nu_bot = bs.nu_bot; out->nu_top = bs.nu_top; out->ntime = bs.ntime; out->status = bs.status;
+  scalars_out(bs, out);
   return 0;
 }
 

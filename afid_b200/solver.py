@@ -126,6 +126,15 @@ class Context:
         f = self._L.afid_step_graph if graph else self._L.afid_step
         _lib.check(f(self.h, ids, n, nsteps))
 
+    def scalars(self, boxes) -> list[dict]:
+        """Box.scalars() of every box of ``boxes``, read with one copy."""
+        ids, n = self._ids(boxes)
+        out = (_lib.BoxScalars * n)()
+        _lib.check(self._L.afid_boxes_get_scalars(self.h, ids, n, out))
+        return [dict(dt=s.dt, time=s.time, cfl=s.cfl, cfl_used=s.cfl_used, divmax=s.divmax,
+                     vmax=tuple(s.vmax), nu_bot=s.nu_bot, nu_top=s.nu_top, ntime=s.ntime,
+                     status=s.status) for s in out]
+
     def step_profiled(self, boxes, nsteps: int = 1) -> dict:
         """Per-kernel device time (ms, summed over nsteps) and launch counts."""
         ids, n = self._ids(boxes)

@@ -460,8 +460,9 @@ def roofline_of(ctx, boxes, cfgs, prof_steps=2, ensemble=False):
 
 def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
     """The same steps through the public C-ABI from pinned host buffers:
-    upload of the initial fields, per step afid_step_graph + the per-box
-    result record (afid_box_get_scalars), download of the final fields."""
+    upload of the initial fields (queued, one wait), per step afid_step_graph
+    + every box's result record (afid_boxes_get_scalars), download of the
+    final fields (queued, one wait)."""
     import ctypes as C
     torch = D.torch
     from afid_b200 import _lib
@@ -478,30 +479,41 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
             ins[k] = t_in          # the final fields overwrite the initial ones
         host.append(ins)
     ids = (C.c_int * len(boxes))(*[b.id for b in boxes])
-    sc = _lib.BoxScalars()
+    sc = _lib.BoxScalars()   # size of one per-box record read back per step
     h2d = sum(5 * cfg.nx * cfg.nym * cfg.nzm * 8 for cfg in cfgs)
     torch.cuda.synchronize()
     D.barrier()
+    recs = (_lib.BoxScalars * len(boxes))()
     t0 = time.perf_counter()
-    for b, ins in zip(boxes, host):
+    for b, ins in zip(boxes, host):     # queued: the copies run back to back on the stream
         for k in fields:
-            _lib.check(L.afid_box_upload(ctx.h, b.id, _lib.FIELDS[k], C.cast(ins[k].data_ptr(), C.POINTER(C.c_double))))
+            _lib.check(L.afid_box_upload_async(ctx.h, b.id, _lib.FIELDS[k],
+                                               C.cast(ins[k].data_ptr(), C.POINTER(C.c_double))))
+    for b in boxes:
         _lib.check(L.afid_box_reset(ctx.h, b.id, 0.0))
+    t1 = time.perf_counter()
     for _ in range(nsteps):
         _lib.check(L.afid_step_graph(ctx.h, ids, len(boxes), 1))
-        for b in boxes:
-            _lib.check(L.afid_box_get_scalars(ctx.h, b.id, C.byref(sc)))
+        _lib.check(L.afid_boxes_get_scalars(ctx.h, ids, len(boxes), recs))   # every box's record
+    t2 = time.perf_counter()
     for b, outs in zip(boxes, host):
         for k in fields:
-            _lib.check(L.afid_box_download(ctx.h, b.id, _lib.FIELDS[k], C.cast(outs[k].data_ptr(), C.POINTER(C.c_double))))
-    t = D.max(time.perf_counter() - t0)
+            _lib.check(L.afid_box_download_async(ctx.h, b.id, _lib.FIELDS[k],
+                                                 C.cast(outs[k].data_ptr(), C.POINTER(C.c_double))))
+    _lib.check(L.afid_ctx_synchronize(ctx.h))
+    t3 = time.perf_counter()
+    t = D.max(t3 - t0)
+    if any(r.status != 0 for r in recs):
+        raise RuntimeError("e2e: a box stopped with a status code")
     ncell = D.sum(sum(cells(c) for c in cfgs))
     return {"value": ncell * nsteps / t / 1e6, "unit": UNIT,
             "h2d_bytes_per_step": D.sum(h2d) / nsteps,
             "d2h_bytes_per_step": D.sum(h2d + C.sizeof(sc) * nsteps * len(boxes)) / nsteps,
-            "what": "afid_box_upload of the initial fields from pinned host memory, K x "
-                    "(afid_step_graph + afid_box_get_scalars of every box), afid_box_download "
-                    "of the final fields"}
+            "split_ms": {"upload_and_reset": round((t1 - t0) * 1e3, 2), "steps": round((t2 - t1) * 1e3, 2),
+                         "download": round((t3 - t2) * 1e3, 2)},
+            "what": "afid_box_upload_async of the initial fields from pinned host memory, K x "
+                    "(afid_step_graph + afid_boxes_get_scalars of every box: one copy and one wait "
+                    "per step), afid_box_download_async of the final fields and afid_ctx_synchronize"}
 
 
 def serve_record(ctx, D: Dist, rate: float, nreq: int, steps: int, quantum: int = 32) -> dict:

@@ -129,6 +129,14 @@ int afid_box_add(afid_ctx *ctx, const afid_box_params *p, const double *xc, int 
 int afid_box_remove(afid_ctx *ctx, int box_id);
 int afid_box_upload(afid_ctx *ctx, int box_id, int field, const double *host);
 int afid_box_download(afid_ctx *ctx, int box_id, int field, double *host);
+/* The same transfers queued on the context's stream, returning at once (no
+ * counterpart in the reference, whose fields live in host memory): the host
+ * buffer must stay valid and unchanged (upload) or unread (download) until
+ * afid_ctx_synchronize or another call that waits for the stream.  From
+ * pinned host memory the copies overlap the caller's other work; transfers of
+ * one box are applied in call order. */
+int afid_box_upload_async(afid_ctx *ctx, int box_id, int field, const double *host);
+int afid_box_download_async(afid_ctx *ctx, int box_id, int field, double *host);
 /* Zero the RK history, the carried rhs wall row, time, step count and
  * status; set dt (values <= 0 keep the current dt). */
 int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
@@ -151,6 +159,10 @@ int afid_box_set_time(afid_ctx *ctx, int box_id, double time);
 int afid_box_interp_field(afid_ctx *ctx, int box_id, int field, const double *old, int nxo, int nyo, int nzo,
                           int istro3, double stro3, int istr3, double str3);
 int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
+/* afid_box_get_scalars of n boxes with one copy and one wait (no counterpart
+ * in the reference): out[q] receives box ids[q]'s record; the set is the
+ * same kind of box set afid_step takes. */
+int afid_boxes_get_scalars(afid_ctx *ctx, const int *box_ids, int n, afid_box_scalars *out);
 /* Hold points of a box (no counterpart in the reference; they move the
  * host's per-step checks of main.F90:207, :256 and :273 onto the device, so
  * that a caller can queue many steps and still stop at the right one).

@@ -133,3 +133,40 @@ def test_batch_tuning_keeps_results(ctx):
             assert np.array_equal(a.download(f), b.download(f)), f
     for b in tuned + plain:
         ctx.remove_box(b)
+
+
+def test_async_transfers_and_batched_scalars(ctx):
+    """afid_box_upload_async / afid_box_download_async queued for several
+    boxes and fields, then one wait, give the same device fields and host
+    arrays as the waiting transfers; afid_boxes_get_scalars gives every
+    box's afid_box_get_scalars record."""
+    from afid_b200 import _lib
+    L = _lib.lib()
+    sync = [_add(ctx, kw, 30 + q) for q, kw in enumerate(MIX)]
+    asyn = [ctx.add_box(b.cfg) for b in sync]
+    keep = []
+    for q, (s, a) in enumerate(zip(sync, asyn)):
+        for k, v in initial_fields(s.cfg, s.xc, 30 + q).items():
+            buf = np.ascontiguousarray(np.asarray(v, dtype=np.float64).transpose(2, 1, 0))
+            keep.append(buf)
+            _lib.check(L.afid_box_upload_async(ctx.h, a.id, _lib.FIELDS[k], _lib.dptr(buf)))
+    ctx.synchronize()
+    ctx.step(sync, 2)
+    ctx.step(asyn, 2)
+    recs = ctx.scalars(asyn)
+    assert recs == [b.scalars() for b in asyn]
+    assert recs == [b.scalars() for b in sync]
+    outs = []
+    for a in asyn:
+        for f in FIELDS:
+            buf = np.empty((a.cfg.nzm, a.cfg.nym, a._rows(f)))
+            outs.append((a, f, buf))
+            _lib.check(L.afid_box_download_async(ctx.h, a.id, _lib.FIELDS[f], _lib.dptr(buf)))
+    ctx.synchronize()
+    for (a, f, buf), s in zip(outs, [s for s in sync for _ in FIELDS]):
+        got = np.ascontiguousarray(buf.transpose(2, 1, 0))
+        assert np.array_equal(got, a.download(f)), f
+        assert np.array_equal(got, s.download(f)), f
+    for b in sync + asyn:
+        ctx.remove_box(b)
+    del keep   # the upload buffers stay alive until the copies have run
