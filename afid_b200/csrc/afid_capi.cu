@@ -87,8 +87,21 @@ struct Batch {
   int grid_wz[WY_NV] = {};          // resident grids of the warp z transforms (shared memory as y)
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
+  int graph_kernels = 0;    // kernel nodes of the captured step graph
   int k1_minb = 4;          // variant of the explicit/forward kernel (tuning, K1_VMIN..K1_VMAX)
+  // A large set is stepped through its graph as two halves of about equal
+  // cells, each with its own graph on its own stream: the halves drift
+  // apart, so that one half's latency-bound transforms run beside the other
+  // half's bandwidth-bound stencils.  The halves are batches of their own
+  // (looked up by their ids, never split again).
+  bool split = false;
+  std::vector<int> half_ids[2];
 };
+
+// splitting rule of afid_step_graph: sets of at least this many boxes and
+// cells run as two halves (AFID_BATCH_STREAMS=1 keeps them whole)
+constexpr int SPLIT_MIN_BOXES = 8;
+constexpr long long SPLIT_MIN_CELLS = 4LL << 20;
 
 long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
 
@@ -381,6 +394,9 @@ struct afid_ctx {
   int next_id = 0;
   std::map<std::vector<int>, Batch *> batches;
   std::vector<double> staging_host;
+  // streams and events of split batches (created on first use)
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   // staging of afid_boxes_get_scalars: device and pinned host records
   BoxScalars *d_sc_stage = nullptr, *h_sc_stage = nullptr;
   int sc_stage_n = 0;
@@ -469,7 +485,7 @@ int k2_block_size(const std::vector<BoxDev> &devs, int *out) {
   return 0;
 }
 
-int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
+int get_batch(afid_ctx *c, const int *ids, int n, Batch **out, bool allow_split = true) {
   if (n <= 0 || !ids) return fail(AFID_EINVAL, "empty box set");
   std::vector<int> key(ids, ids + n);
   auto it = c->batches.find(key);
@@ -528,6 +544,28 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out) {
     if (!rc) rc = fft_grid(k_fft_z<-1>, bt->smem_z, bt->total[FAM_FZ], &bt->grid_z);
     if (!rc) rc = wy_shapes(devs, bt->total, bt->smem_wy, bt->grid_wy, bt->grid_wz);
     if (rc) { free_batch(bt); return rc; }
+  }
+  if (allow_split && n >= SPLIT_MIN_BOXES) {
+    const char *e = getenv("AFID_BATCH_STREAMS");
+    long long cells = 0;
+    for (const BoxDev &d : devs) cells += (long long)d.nxm * d.plane;
+    if (cells >= SPLIT_MIN_CELLS && !(e && atoi(e) == 1)) {
+      // greedy balance of cells, largest boxes first; each half keeps the
+      // set's order
+      std::vector<int> order(n), side(n, 0);
+      for (int b = 0; b < n; ++b) order[b] = b;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (long long)devs[a].nxm * devs[a].plane > (long long)devs[b].nxm * devs[b].plane;
+      });
+      long long load[2] = {0, 0};
+      for (int b : order) {
+        const int h = load[1] < load[0] ? 1 : 0;
+        side[b] = h;
+        load[h] += (long long)devs[b].nxm * devs[b].plane;
+      }
+      for (int b = 0; b < n; ++b) bt->half_ids[side[b]].push_back(ids[b]);
+      bt->split = !bt->half_ids[0].empty() && !bt->half_ids[1].empty();
+    }
   }
   c->batches[key] = bt;
   *out = bt;
@@ -857,7 +895,14 @@ int afid_ctx_destroy(afid_ctx *c) {
   if (!c) return 0;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  for (int h = 0; h < 2; ++h)
+    if (c->side[h]) cudaStreamSynchronize(c->side[h]);
   for (auto &kv : c->batches) free_batch(kv.second);
+  for (int h = 0; h < 2; ++h) {
+    if (c->side[h]) cudaStreamDestroy(c->side[h]);
+    if (c->ev_join[h]) cudaEventDestroy(c->ev_join[h]);
+  }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->d_sc_stage) cudaFree(c->d_sc_stage);
   if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
   for (auto &kv : c->boxes) {
@@ -1611,6 +1656,64 @@ int afid_step_profiled(afid_ctx *c, const int *ids, int n, int nsteps, double *k
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The step graph of batch bt for stream st (captured on first use, and
+// again when the stream changes).
+int ensure_graph(Batch *bt, cudaStream_t st) {
+  if (bt->gexec && bt->gstream == st) return 0;
+  if (bt->gexec) { cudaGraphExecDestroy(bt->gexec); bt->gexec = nullptr; }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int rc = launch_step(bt, st);
+  cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(AFID_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+  size_t nn = 0;
+  e = cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+  int nk = 0;
+  for (size_t q = 0; e == cudaSuccess && q < nn; ++q) {
+    cudaGraphNodeType t;
+    e = cudaGraphNodeGetType(nodes[q], &t);
+    if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nk;
+  }
+  if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(AFID_ECUDA, "graph nodes: %s", cudaGetErrorString(e)); }
+  e = cudaGraphInstantiate(&bt->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { bt->gexec = nullptr; return fail(AFID_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+  bt->gstream = st;
+  bt->graph_kernels = nk;
+  return 0;
+}
+
+// The streams and events of split batches.
+int ensure_side(afid_ctx *c) {
+  for (int h = 0; h < 2; ++h)
+    if (!c->side[h]) CK(cudaStreamCreateWithFlags(&c->side[h], cudaStreamNonBlocking));
+  if (!c->ev_fork) CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  for (int h = 0; h < 2; ++h)
+    if (!c->ev_join[h]) CK(cudaEventCreateWithFlags(&c->ev_join[h], cudaEventDisableTiming));
+  return 0;
+}
+
+// The halves of a split batch with their graphs on the side streams.
+int split_halves(afid_ctx *c, const Batch *bt, Batch **hb) {
+  int rc = ensure_side(c);
+  for (int h = 0; !rc && h < 2; ++h) {
+    rc = get_batch(c, bt->half_ids[h].data(), (int)bt->half_ids[h].size(), &hb[h], false);
+    if (!rc) rc = ensure_graph(hb[h], c->side[h]);
+  }
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
 int afid_step_graph(afid_ctx *c, const int *ids, int n, int nsteps) {
   if (!c) return fail(AFID_EINVAL, "null ctx");
   if (nsteps < 0) return fail(AFID_EINVAL, "nsteps < 0");
@@ -1619,20 +1722,46 @@ int afid_step_graph(afid_ctx *c, const int *ids, int n, int nsteps) {
   Batch *bt;
   rc = get_batch(c, ids, n, &bt);
   if (rc) return rc;
-  if (!bt->gexec || bt->gstream != c->stream) {
-    if (bt->gexec) { cudaGraphExecDestroy(bt->gexec); bt->gexec = nullptr; }
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    rc = launch_step(bt, c->stream);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (bt->split) {
+    // each half steps on its own stream between a fork from and a join to
+    // the context's stream; the halves are independent, so they need no
+    // other ordering
+    Batch *hb[2];
+    rc = split_halves(c, bt, hb);
     if (rc) return rc;
-    if (e != cudaSuccess) return fail(AFID_ECUDA, "graph capture: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&bt->gexec, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) { bt->gexec = nullptr; return fail(AFID_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
-    bt->gstream = c->stream;
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    for (int h = 0; h < 2; ++h) CK(cudaStreamWaitEvent(c->side[h], c->ev_fork, 0));
+    for (int s = 0; s < nsteps; ++s)
+      for (int h = 0; h < 2; ++h) CK(cudaGraphLaunch(hb[h]->gexec, c->side[h]));
+    for (int h = 0; h < 2; ++h) {
+      CK(cudaEventRecord(c->ev_join[h], c->side[h]));
+      CK(cudaStreamWaitEvent(c->stream, c->ev_join[h], 0));
+    }
+    return 0;
   }
+  rc = ensure_graph(bt, c->stream);
+  if (rc) return rc;
   for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(bt->gexec, c->stream));
+  return 0;
+}
+
+int afid_step_graph_kernels(afid_ctx *c, const int *ids, int n, int *kernels) {
+  if (!c || !kernels) return fail(AFID_EINVAL, "null argument");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  if (bt->split) {
+    Batch *hb[2];
+    rc = split_halves(c, bt, hb);
+    if (rc) return rc;
+    *kernels = hb[0]->graph_kernels + hb[1]->graph_kernels;
+    return 0;
+  }
+  rc = ensure_graph(bt, c->stream);
+  if (rc) return rc;
+  *kernels = bt->graph_kernels;
   return 0;
 }
 

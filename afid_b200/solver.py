@@ -126,6 +126,13 @@ class Context:
         f = self._L.afid_step_graph if graph else self._L.afid_step
         _lib.check(f(self.h, ids, n, nsteps))
 
+    def graph_kernels(self, boxes) -> int:
+        """Kernels one graph step of ``boxes`` launches (see Context.step)."""
+        ids, n = self._ids(boxes)
+        k = C.c_int(0)
+        _lib.check(self._L.afid_step_graph_kernels(self.h, ids, n, C.byref(k)))
+        return k.value
+
     def scalars(self, boxes) -> list[dict]:
         """Box.scalars() of every box of ``boxes``, read with one copy."""
         ids, n = self._ids(boxes)

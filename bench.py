@@ -603,6 +603,7 @@ def gpu_arm(args):
     # warm-up (also captures the CUDA graph of one step)
     ctx.step(boxes, max(args.warmup, 1), graph=True)
     ctx.synchronize()
+    graph_kernels = ctx.graph_kernels(boxes)   # kernels of one timed step (both halves of a split set)
 
     # ---- timed region: K steps through the captured graph, device events
     clocks = ClockSampler(device)
@@ -613,7 +614,7 @@ def gpu_arm(args):
     statuses = [b.scalars()["status"] for b in boxes]
     div_max = max(max(h["divmax"] for h in b.history(args.steps)) for b in boxes)
 
-    roof, launches_per_step = roofline_of(ctx, boxes, cfgs, ensemble=(args.workload == "batch"))
+    roof, _ = roofline_of(ctx, boxes, cfgs, ensemble=(args.workload == "batch"))
     e2e = e2e_run(ctx, boxes, cfgs, seeds, args.steps, D)
 
     batched = None
@@ -670,7 +671,7 @@ def gpu_arm(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": conf, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(round(launches_per_step * args.steps)), "clocks": clk,
+            "gpu_launches": int(graph_kernels * args.steps), "clocks": clk,
             "status": statuses, "max_divergence_timed": div_max,
         }
         if batched is not None:

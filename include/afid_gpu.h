@@ -222,9 +222,17 @@ int afid_calc_plate_nu(afid_ctx *ctx, int box_id, double *nuslow, double *nusupp
  * afid_step: nsteps passes of main.F90:171-200 (CalcMaxCFL, dt rule,
  * TimeMarcher, time += dt, CalcPlateNu) for every listed box, each kernel
  * launched once for all boxes.  afid_step_graph does the same through a
- * CUDA graph of one step, captured on first use per box set. */
+ * CUDA graph of one step, captured on first use per box set.  A set of at
+ * least 8 boxes and 4 Mi cells runs there as two halves of about equal
+ * cells, each with its own graph on a stream of the context, forked from
+ * and joined back to the context's stream (AFID_BATCH_STREAMS=1 in the
+ * environment keeps sets whole); the results are the same either way. */
 int afid_step(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
 int afid_step_graph(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
+/* Kernels one afid_step_graph step of this set launches (both halves of a
+ * split set); captures the graphs if needed (no counterpart in the
+ * reference). */
+int afid_step_graph_kernels(afid_ctx *ctx, const int *box_ids, int nbox, int *kernels);
 /* One substep ns of TimeMarcher.F90:28-72 with the current dt (no CFL). */
 int afid_substep(afid_ctx *ctx, const int *box_ids, int nbox, int ns);
 

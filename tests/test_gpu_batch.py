@@ -170,3 +170,24 @@ def test_async_transfers_and_batched_scalars(ctx):
     for b in sync + asyn:
         ctx.remove_box(b)
     del keep   # the upload buffers stay alive until the copies have run
+
+
+def test_split_graph_equals_direct(ctx):
+    """A set large enough for afid_step_graph to run it as two halves on two
+    streams gives bit for bit the fields and records of the same set
+    stepped by direct launches, and its graph step launches both halves'
+    kernels."""
+    kws = [dict(nxm=64, nym=96, nzm=96, ray=10 ** (5 + 0.4 * q), pra=(0.7, 1.0, 4.38)[q % 3], dt=1e-4)
+           for q in range(8)]
+    graphed = [_add(ctx, kw, 50 + q) for q, kw in enumerate(kws)]
+    direct = [_add(ctx, kw, 50 + q) for q, kw in enumerate(kws)]
+    ctx.step(graphed, 3, graph=True)
+    ctx.step(direct, 3)
+    for g, d in zip(graphed, direct):
+        for f in FIELDS:
+            assert np.array_equal(g.download(f), d.download(f)), f
+        assert g.scalars() == d.scalars()
+    one = ctx.graph_kernels(graphed[:1])
+    assert ctx.graph_kernels(graphed) > one
+    for b in graphed + direct:
+        ctx.remove_box(b)
