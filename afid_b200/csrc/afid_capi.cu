@@ -1305,6 +1305,18 @@ __global__ void k_gather_scalars(const BoxDev *boxes, int n, BoxScalars *dst) {
   if (b < n) dst[b] = *boxes[b].sc;
 }
 
+// the public records of n boxes, written straight in afid_box_scalars layout
+__global__ void k_gather_records(const BoxDev *boxes, int n, afid_box_scalars *dst) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const BoxScalars &bs = *boxes[b].sc;
+  afid_box_scalars o;
+  o.dt = bs.dt; o.time = bs.time; o.cfl = bs.cfl; o.cfl_used = bs.cfl_used; o.divmax = bs.divmax;
+  for (int q = 0; q < 3; ++q) o.vmax[q] = bs.vmax[q];
+  o.nu_bot = bs.nu_bot; o.nu_top = bs.nu_top; o.ntime = bs.ntime; o.status = bs.status;
+  dst[b] = o;
+}
+
 int afid_boxes_get_scalars(afid_ctx *c, const int *ids, int n, afid_box_scalars *out) {
   if (!c || !ids || !out || n <= 0) return fail(AFID_EINVAL, "boxes_get_scalars: null argument or n <= 0");
   int rc = set_device(c);
@@ -1328,6 +1340,36 @@ int afid_boxes_get_scalars(afid_ctx *c, const int *ids, int n, afid_box_scalars 
   CK(cudaMemcpyAsync(c->h_sc_stage, c->d_sc_stage, sizeof(BoxScalars) * n, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   for (int b = 0; b < n; ++b) scalars_out(c->h_sc_stage[b], out + b);
+  return 0;
+}
+
+int afid_boxes_get_scalars_async(afid_ctx *c, const int *ids, int n, afid_box_scalars *out) {
+  if (!c || !ids || !out || n <= 0) return fail(AFID_EINVAL, "boxes_get_scalars_async: null argument or n <= 0");
+  int rc = set_device(c);
+  if (rc) return rc;
+  Batch *bt;
+  rc = get_batch(c, ids, n, &bt);
+  if (rc) return rc;
+  // one device staging array serves every call: each call's copy is queued
+  // right behind its gather, and the next call's gather behind that copy,
+  // so no record is overwritten before it is copied
+  const size_t need = (sizeof(afid_box_scalars) * n + sizeof(BoxScalars) - 1) / sizeof(BoxScalars);
+  if ((int)need > c->sc_stage_n) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->d_sc_stage) cudaFree(c->d_sc_stage);
+    if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
+    c->d_sc_stage = nullptr;
+    c->h_sc_stage = nullptr;
+    c->sc_stage_n = 0;
+    if (cudaMalloc(&c->d_sc_stage, sizeof(BoxScalars) * need) != cudaSuccess ||
+        cudaMallocHost(&c->h_sc_stage, sizeof(BoxScalars) * need) != cudaSuccess)
+      return fail(AFID_ENOMEM, "boxes_get_scalars_async: staging of %d records", n);
+    c->sc_stage_n = (int)need;
+  }
+  afid_box_scalars *d = reinterpret_cast<afid_box_scalars *>(c->d_sc_stage);
+  k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, d);
+  CKL();
+  CK(cudaMemcpyAsync(out, d, sizeof(afid_box_scalars) * n, cudaMemcpyDeviceToHost, c->stream));
   return 0;
 }
 

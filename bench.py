@@ -460,9 +460,10 @@ def roofline_of(ctx, boxes, cfgs, prof_steps=2, ensemble=False):
 
 def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
     """The same steps through the public C-ABI from pinned host buffers:
-    upload of the initial fields (queued, one wait), per step afid_step_graph
-    + every box's result record (afid_boxes_get_scalars), download of the
-    final fields (queued, one wait)."""
+    upload of the initial fields (queued), per step afid_step_graph + every
+    box's result record copied back into that step's slot of a pinned buffer
+    (afid_boxes_get_scalars_async), download of the final fields (queued),
+    one wait at the end."""
     import ctypes as C
     torch = D.torch
     from afid_b200 import _lib
@@ -483,7 +484,11 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
     h2d = sum(5 * cfg.nx * cfg.nym * cfg.nzm * 8 for cfg in cfgs)
     torch.cuda.synchronize()
     D.barrier()
-    recs = (_lib.BoxScalars * len(boxes))()
+    # one pinned slot of records per step: each step's records are copied back
+    # behind that step, and read on the host after the final wait
+    nb = len(boxes)
+    rec_buf = torch.empty(nsteps * nb * C.sizeof(_lib.BoxScalars), dtype=torch.uint8, pin_memory=True)
+    recs = (_lib.BoxScalars * (nsteps * nb)).from_address(rec_buf.data_ptr())
     t0 = time.perf_counter()
     for b, ins in zip(boxes, host):     # queued: the copies run back to back on the stream
         for k in fields:
@@ -492,10 +497,10 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
     for b in boxes:
         _lib.check(L.afid_box_reset(ctx.h, b.id, 0.0))
     t1 = time.perf_counter()
-    for _ in range(nsteps):
-        _lib.check(L.afid_step_graph(ctx.h, ids, len(boxes), 1))
-        _lib.check(L.afid_boxes_get_scalars(ctx.h, ids, len(boxes), recs))   # every box's record
-    t2 = time.perf_counter()
+    for s in range(nsteps):
+        _lib.check(L.afid_step_graph(ctx.h, ids, nb, 1))
+        slot = C.cast(C.addressof(recs) + s * nb * C.sizeof(_lib.BoxScalars), C.POINTER(_lib.BoxScalars))
+        _lib.check(L.afid_boxes_get_scalars_async(ctx.h, ids, nb, slot))
     for b, outs in zip(boxes, host):
         for k in fields:
             _lib.check(L.afid_box_download_async(ctx.h, b.id, _lib.FIELDS[k],
@@ -503,17 +508,19 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
     _lib.check(L.afid_ctx_synchronize(ctx.h))
     t3 = time.perf_counter()
     t = D.max(t3 - t0)
-    if any(r.status != 0 for r in recs):
-        raise RuntimeError("e2e: a box stopped with a status code")
+    if any(recs[(nsteps - 1) * nb + q].status != 0 for q in range(nb)) or \
+            any(recs[s * nb].ntime != recs[0].ntime + s for s in range(nsteps)):
+        raise RuntimeError("e2e: a box stopped with a status code, or a record is missing")
     ncell = D.sum(sum(cells(c) for c in cfgs))
     return {"value": ncell * nsteps / t / 1e6, "unit": UNIT,
             "h2d_bytes_per_step": D.sum(h2d) / nsteps,
             "d2h_bytes_per_step": D.sum(h2d + C.sizeof(sc) * nsteps * len(boxes)) / nsteps,
-            "split_ms": {"upload_and_reset": round((t1 - t0) * 1e3, 2), "steps": round((t2 - t1) * 1e3, 2),
-                         "download": round((t3 - t2) * 1e3, 2)},
+            "split_ms": {"upload_and_reset": round((t1 - t0) * 1e3, 2),
+                         "steps_records_download": round((t3 - t1) * 1e3, 2)},
             "what": "afid_box_upload_async of the initial fields from pinned host memory, K x "
-                    "(afid_step_graph + afid_boxes_get_scalars of every box: one copy and one wait "
-                    "per step), afid_box_download_async of the final fields and afid_ctx_synchronize"}
+                    "(afid_step_graph + afid_boxes_get_scalars_async: every box's record of that step "
+                    "copied to pinned host memory), afid_box_download_async of the final fields, "
+                    "afid_ctx_synchronize"}
 
 
 def serve_record(ctx, D: Dist, rate: float, nreq: int, steps: int, quantum: int = 32) -> dict:

@@ -163,6 +163,12 @@ int afid_box_get_scalars(afid_ctx *ctx, int box_id, afid_box_scalars *out);
  * in the reference): out[q] receives box ids[q]'s record; the set is the
  * same kind of box set afid_step takes. */
 int afid_boxes_get_scalars(afid_ctx *ctx, const int *box_ids, int n, afid_box_scalars *out);
+/* The same records queued on the context's stream, returning at once (no
+ * counterpart in the reference): out[0..n) is filled once the stream gets
+ * there (after afid_ctx_synchronize at the latest) and must stay valid
+ * until then; from pinned host memory the copy overlaps later queued work.
+ * Each call's records are those of the boxes at that point of the stream. */
+int afid_boxes_get_scalars_async(afid_ctx *ctx, const int *box_ids, int n, afid_box_scalars *out);
 /* Hold points of a box (no counterpart in the reference; they move the
  * host's per-step checks of main.F90:207, :256 and :273 onto the device, so
  * that a caller can queue many steps and still stop at the right one).

@@ -156,6 +156,20 @@ def test_async_transfers_and_batched_scalars(ctx):
     recs = ctx.scalars(asyn)
     assert recs == [b.scalars() for b in asyn]
     assert recs == [b.scalars() for b in sync]
+    # queued records: one slot per step, read after one wait
+    import ctypes as C
+    ids = (C.c_int * len(asyn))(*[b.id for b in asyn])
+    slots = (_lib.BoxScalars * (2 * len(asyn)))()
+    for q in range(2):
+        ctx.step(asyn, 1)
+        ptr = C.cast(C.addressof(slots) + q * len(asyn) * C.sizeof(_lib.BoxScalars), C.POINTER(_lib.BoxScalars))
+        _lib.check(L.afid_boxes_get_scalars_async(ctx.h, ids, len(asyn), ptr))
+    ctx.synchronize()
+    assert [slots[len(asyn) + q].ntime for q in range(len(asyn))] == [r["ntime"] + 2 for r in recs]
+    assert [slots[q].ntime for q in range(len(asyn))] == [r["ntime"] + 1 for r in recs]
+    last = ctx.scalars(asyn)
+    assert [slots[len(asyn) + q].time for q in range(len(asyn))] == [r["time"] for r in last]
+    ctx.step(sync, 2)
     outs = []
     for a in asyn:
         for f in FIELDS:
