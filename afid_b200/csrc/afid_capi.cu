@@ -398,8 +398,13 @@ struct afid_ctx {
   cudaStream_t side[2] = {nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   // staging of afid_boxes_get_scalars: device and pinned host records
-  BoxScalars *d_sc_stage = nullptr, *h_sc_stage = nullptr;
-  int sc_stage_n = 0;
+  // (one per stream the context has used, so that calls on different
+  // streams never share a staging array)
+  struct RecStage {
+    BoxScalars *d = nullptr, *h = nullptr;
+    int n = 0;     // records of BoxScalars size it holds
+  };
+  std::map<cudaStream_t, RecStage> rec_stage;
 };
 
 namespace {
@@ -903,8 +908,10 @@ int afid_ctx_destroy(afid_ctx *c) {
     if (c->ev_join[h]) cudaEventDestroy(c->ev_join[h]);
   }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-  if (c->d_sc_stage) cudaFree(c->d_sc_stage);
-  if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
+  for (auto &kv : c->rec_stage) {
+    if (kv.second.d) cudaFree(kv.second.d);
+    if (kv.second.h) cudaFreeHost(kv.second.h);
+  }
   for (auto &kv : c->boxes) {
     HostBox *hb = kv.second;
     cudaFree(hb->mem_fields); cudaFree(hb->mem_scratch); cudaFree(hb->mem_small);
@@ -1169,6 +1176,15 @@ int afid_box_download_async(afid_ctx *c, int id, int field, double *host) {
   return transfer(c, id, field, host, false, false);
 }
 
+__global__ void k_reset_scalars(BoxScalars *S, double dt) {
+  S->time = 0.0;
+  S->ntime = 0;
+  S->status = 0;
+  S->nonfinite = 0;
+  for (int q = 0; q < 4; ++q) S->red_u64[q] = 0ull;
+  if (dt > 0) S->dt = dt;
+}
+
 int afid_box_reset(afid_ctx *c, int id, double dt) {
   if (!c) return fail(AFID_EINVAL, "null ctx");
   HostBox *hb;
@@ -1180,14 +1196,9 @@ int afid_box_reset(afid_ctx *c, int id, double dt) {
   cudaStream_t st = c->stream;
   CK(cudaMemsetAsync(d.rux, 0, 4 * (size_t)d.fsize * sizeof(double), st));
   CK(cudaMemsetAsync(d.wall, 0, (size_t)d.plane * sizeof(double), st));
-  BoxScalars bs;
-  CK(cudaMemcpyAsync(&bs, d.sc, sizeof bs, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  bs.time = 0.0; bs.ntime = 0; bs.status = 0; bs.nonfinite = 0;
-  for (int q = 0; q < 4; ++q) bs.red_u64[q] = 0;
-  if (dt > 0) bs.dt = dt;
-  CK(cudaMemcpyAsync(d.sc, &bs, sizeof bs, cudaMemcpyHostToDevice, st));
-  CK(cudaStreamSynchronize(st));
+  // the record on the device, in stream order (no host round trip)
+  k_reset_scalars<<<1, 1, 0, st>>>(d.sc, dt);
+  CKL();
   return 0;
 }
 
@@ -1293,6 +1304,30 @@ int afid_box_interp_field(afid_ctx *c, int id, int field, const double *old, int
   return 0;
 }
 
+// The record staging of the context's current stream, grown to n records
+// (growing waits for the stream first: a queued copy may still read it).
+// The pinned host half is made only when a caller needs it (the waiting
+// read): allocating pinned memory can stall the whole device, which the
+// queued read must not do after its first call on a stream.
+static int rec_stage(afid_ctx *c, int n, bool host, afid_ctx::RecStage **out) {
+  afid_ctx::RecStage &rs = c->rec_stage[c->stream];
+  if (n > rs.n || (host && !rs.h)) {
+    CK(cudaStreamSynchronize(c->stream));
+    const int m = n > rs.n ? n : rs.n;
+    if (rs.d) cudaFree(rs.d);
+    if (rs.h) cudaFreeHost(rs.h);
+    rs.d = nullptr;
+    rs.h = nullptr;
+    rs.n = 0;
+    if (cudaMalloc(&rs.d, sizeof(BoxScalars) * m) != cudaSuccess ||
+        (host && cudaMallocHost(&rs.h, sizeof(BoxScalars) * m) != cudaSuccess))
+      return fail(AFID_ENOMEM, "record staging of %d records", m);
+    rs.n = m;
+  }
+  *out = &rs;
+  return 0;
+}
+
 static void scalars_out(const BoxScalars &bs, afid_box_scalars *out) {
   out->dt = bs.dt; out->time = bs.time; out->cfl = bs.cfl; out->cfl_used = bs.cfl_used;
   out->divmax = bs.divmax;
@@ -1324,22 +1359,14 @@ int afid_boxes_get_scalars(afid_ctx *c, const int *ids, int n, afid_box_scalars 
   Batch *bt;
   rc = get_batch(c, ids, n, &bt);
   if (rc) return rc;
-  if (n > c->sc_stage_n) {
-    if (c->d_sc_stage) cudaFree(c->d_sc_stage);
-    if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
-    c->d_sc_stage = nullptr;
-    c->h_sc_stage = nullptr;
-    c->sc_stage_n = 0;
-    if (cudaMalloc(&c->d_sc_stage, sizeof(BoxScalars) * n) != cudaSuccess ||
-        cudaMallocHost(&c->h_sc_stage, sizeof(BoxScalars) * n) != cudaSuccess)
-      return fail(AFID_ENOMEM, "boxes_get_scalars: staging of %d records", n);
-    c->sc_stage_n = n;
-  }
-  k_gather_scalars<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, c->d_sc_stage);
+  afid_ctx::RecStage *rs;
+  rc = rec_stage(c, n, true, &rs);
+  if (rc) return rc;
+  k_gather_scalars<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, rs->d);
   CKL();
-  CK(cudaMemcpyAsync(c->h_sc_stage, c->d_sc_stage, sizeof(BoxScalars) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(rs->h, rs->d, sizeof(BoxScalars) * n, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int b = 0; b < n; ++b) scalars_out(c->h_sc_stage[b], out + b);
+  for (int b = 0; b < n; ++b) scalars_out(rs->h[b], out + b);
   return 0;
 }
 
@@ -1350,23 +1377,14 @@ int afid_boxes_get_scalars_async(afid_ctx *c, const int *ids, int n, afid_box_sc
   Batch *bt;
   rc = get_batch(c, ids, n, &bt);
   if (rc) return rc;
-  // one device staging array serves every call: each call's copy is queued
-  // right behind its gather, and the next call's gather behind that copy,
-  // so no record is overwritten before it is copied
+  // the stream's staging array serves every call on it: each call's copy is
+  // queued right behind its gather, and the next call's gather behind that
+  // copy, so no record is overwritten before it is copied
   const size_t need = (sizeof(afid_box_scalars) * n + sizeof(BoxScalars) - 1) / sizeof(BoxScalars);
-  if ((int)need > c->sc_stage_n) {
-    CK(cudaStreamSynchronize(c->stream));
-    if (c->d_sc_stage) cudaFree(c->d_sc_stage);
-    if (c->h_sc_stage) cudaFreeHost(c->h_sc_stage);
-    c->d_sc_stage = nullptr;
-    c->h_sc_stage = nullptr;
-    c->sc_stage_n = 0;
-    if (cudaMalloc(&c->d_sc_stage, sizeof(BoxScalars) * need) != cudaSuccess ||
-        cudaMallocHost(&c->h_sc_stage, sizeof(BoxScalars) * need) != cudaSuccess)
-      return fail(AFID_ENOMEM, "boxes_get_scalars_async: staging of %d records", n);
-    c->sc_stage_n = (int)need;
-  }
-  afid_box_scalars *d = reinterpret_cast<afid_box_scalars *>(c->d_sc_stage);
+  afid_ctx::RecStage *rs;
+  rc = rec_stage(c, (int)need, false, &rs);
+  if (rc) return rc;
+  afid_box_scalars *d = reinterpret_cast<afid_box_scalars *>(rs->d);
   k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, d);
   CKL();
   CK(cudaMemcpyAsync(out, d, sizeof(afid_box_scalars) * n, cudaMemcpyDeviceToHost, c->stream));

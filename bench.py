@@ -496,7 +496,6 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
                                                C.cast(ins[k].data_ptr(), C.POINTER(C.c_double))))
     for b in boxes:
         _lib.check(L.afid_box_reset(ctx.h, b.id, 0.0))
-    t1 = time.perf_counter()
     for s in range(nsteps):
         _lib.check(L.afid_step_graph(ctx.h, ids, nb, 1))
         slot = C.cast(C.addressof(recs) + s * nb * C.sizeof(_lib.BoxScalars), C.POINTER(_lib.BoxScalars))
@@ -515,8 +514,6 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
     return {"value": ncell * nsteps / t / 1e6, "unit": UNIT,
             "h2d_bytes_per_step": D.sum(h2d) / nsteps,
             "d2h_bytes_per_step": D.sum(h2d + C.sizeof(sc) * nsteps * len(boxes)) / nsteps,
-            "split_ms": {"upload_and_reset": round((t1 - t0) * 1e3, 2),
-                         "steps_records_download": round((t3 - t1) * 1e3, 2)},
             "what": "afid_box_upload_async of the initial fields from pinned host memory, K x "
                     "(afid_step_graph + afid_boxes_get_scalars_async: every box's record of that step "
                     "copied to pinned host memory), afid_box_download_async of the final fields, "

@@ -138,7 +138,8 @@ int afid_box_download(afid_ctx *ctx, int box_id, int field, double *host);
 int afid_box_upload_async(afid_ctx *ctx, int box_id, int field, const double *host);
 int afid_box_download_async(afid_ctx *ctx, int box_id, int field, double *host);
 /* Zero the RK history, the carried rhs wall row, time, step count and
- * status; set dt (values <= 0 keep the current dt). */
+ * status; set dt (values <= 0 keep the current dt).  Queued on the
+ * context's stream (the host does not wait). */
 int afid_box_reset(afid_ctx *ctx, int box_id, double dt);
 /* Set the simulation time (the time a restart reads from the continua
  * master record, ReadFlowField.F90:24-40). */

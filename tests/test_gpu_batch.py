@@ -205,3 +205,40 @@ def test_split_graph_equals_direct(ctx):
     assert ctx.graph_kernels(graphed) > one
     for b in graphed + direct:
         ctx.remove_box(b)
+
+
+def test_queued_records_on_two_streams(ctx):
+    """Two box sets stepped and read back on two streams of one context,
+    queued one after the other with no wait between: each stream's records
+    are its own set's (the record staging is per stream), and a queued
+    reset takes effect in stream order."""
+    import ctypes as C
+
+    import torch
+
+    from afid_b200 import _lib
+    L = _lib.lib()
+    sets = [[_add(ctx, kw, 70 + 10 * h + q) for q, kw in enumerate(MIX[:2])] for h in range(2)]
+    streams = [torch.cuda.Stream() for _ in sets]
+    own = ctx.stream
+    slots = [(_lib.BoxScalars * 2)() for _ in sets]
+    try:
+        for h, (boxes, st) in enumerate(zip(sets, streams)):
+            ctx.set_stream(st.cuda_stream)
+            ids = (C.c_int * 2)(*[b.id for b in boxes])
+            if h == 1:
+                for b in boxes:
+                    b.reset(2e-5)
+            ctx.step(boxes, 2 + h)
+            _lib.check(L.afid_boxes_get_scalars_async(ctx.h, ids, 2, slots[h]))
+        for st in streams:
+            st.synchronize()
+    finally:
+        ctx.set_stream(own)
+    for h, boxes in enumerate(sets):
+        want = ctx.scalars(boxes)
+        assert [slots[h][q].ntime for q in range(2)] == [r["ntime"] for r in want] == [2 + h] * 2
+        assert [slots[h][q].time for q in range(2)] == [r["time"] for r in want]
+    assert all(r["dt"] == 2e-5 for r in ctx.scalars(sets[1]))
+    for b in sets[0] + sets[1]:
+        ctx.remove_box(b)
