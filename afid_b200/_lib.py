@@ -29,7 +29,7 @@ EXPORTS = [
     "afid_box_device_bytes", "afid_box_add", "afid_box_remove", "afid_box_upload",
     "afid_box_download", "afid_box_reset", "afid_box_get_scalars", "afid_box_history",
     "afid_box_upload_async", "afid_box_download_async", "afid_boxes_get_scalars",
-    "afid_step_graph_kernels", "afid_boxes_get_scalars_async",
+    "afid_step_graph_kernels", "afid_boxes_get_scalars_async", "afid_ctx_set_split_sets",
     "afid_time_marcher_begin_substep", "afid_explicit_terms_vx", "afid_explicit_terms_vy",
     "afid_explicit_terms_vz", "afid_explicit_terms_temp", "afid_implicit_and_update_vx",
     "afid_implicit_and_update_vy", "afid_implicit_and_update_vz",
@@ -120,6 +120,7 @@ def lib(path: str | None = None) -> C.CDLL:
         "afid_boxes_get_scalars": ([vp, ip, i, C.POINTER(BoxScalars)], i),
         "afid_step_graph_kernels": ([vp, ip, i, ip], i),
         "afid_boxes_get_scalars_async": ([vp, ip, i, C.POINTER(BoxScalars)], i),
+        "afid_ctx_set_split_sets": ([vp, i], i),
         "afid_box_reset": ([vp, i, d], i),
         "afid_box_get_scalars": ([vp, i, C.POINTER(BoxScalars)], i),
         "afid_box_history": ([vp, i, C.POINTER(StepRecord), i], i),

@@ -99,7 +99,7 @@ struct Batch {
 };
 
 // splitting rule of afid_step_graph: sets of at least this many boxes and
-// cells run as two halves (AFID_BATCH_STREAMS=1 keeps them whole)
+// cells run as two halves (afid_ctx_set_split_sets turns it off)
 constexpr int SPLIT_MIN_BOXES = 8;
 constexpr long long SPLIT_MIN_CELLS = 4LL << 20;
 
@@ -394,7 +394,9 @@ struct afid_ctx {
   int next_id = 0;
   std::map<std::vector<int>, Batch *> batches;
   std::vector<double> staging_host;
-  // streams and events of split batches (created on first use)
+  // streams and events of split batches (created on first use); split_sets
+  // 0 keeps every set whole (afid_ctx_set_split_sets)
+  int split_sets = 1;
   cudaStream_t side[2] = {nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   // staging of afid_boxes_get_scalars: device and pinned host records
@@ -551,10 +553,9 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out, bool allow_split 
     if (rc) { free_batch(bt); return rc; }
   }
   if (allow_split && n >= SPLIT_MIN_BOXES) {
-    const char *e = getenv("AFID_BATCH_STREAMS");
     long long cells = 0;
     for (const BoxDev &d : devs) cells += (long long)d.nxm * d.plane;
-    if (cells >= SPLIT_MIN_CELLS && !(e && atoi(e) == 1)) {
+    if (cells >= SPLIT_MIN_CELLS) {
       // greedy balance of cells, largest boxes first; each half keeps the
       // set's order
       std::vector<int> order(n), side(n, 0);
@@ -890,6 +891,10 @@ int afid_ctx_create(afid_ctx **out, int device) {
     return fail(AFID_ECUDA, "ctx create: %s", cudaGetErrorString(e));
   }
   c->stream = c->own;
+  {
+    const char *e = getenv("AFID_BATCH_STREAMS");
+    if (e && atoi(e) == 1) c->split_sets = 0;
+  }
   int rc = init_kernel_attrs();
   if (rc) { cudaStreamDestroy(c->own); delete c; return rc; }
   *out = c;
@@ -920,6 +925,12 @@ int afid_ctx_destroy(afid_ctx *c) {
   }
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
+  return 0;
+}
+
+int afid_ctx_set_split_sets(afid_ctx *c, int on) {
+  if (!c) return fail(AFID_EINVAL, "null ctx");
+  c->split_sets = on ? 1 : 0;
   return 0;
 }
 
@@ -1176,13 +1187,20 @@ int afid_box_download_async(afid_ctx *c, int id, int field, double *host) {
   return transfer(c, id, field, host, false, false);
 }
 
-__global__ void k_reset_scalars(BoxScalars *S, double dt) {
-  S->time = 0.0;
-  S->ntime = 0;
-  S->status = 0;
-  S->nonfinite = 0;
-  for (int q = 0; q < 4; ++q) S->red_u64[q] = 0ull;
-  if (dt > 0) S->dt = dt;
+__global__ void k_reset_box(double *hist, long long nh, double *wall, long long nw, BoxScalars *S, double dt) {
+  const long long n = nh + nw;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    if (e < nh) hist[e] = 0.0;
+    else wall[e - nh] = 0.0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->time = 0.0;
+    S->ntime = 0;
+    S->status = 0;
+    S->nonfinite = 0;
+    for (int q = 0; q < 4; ++q) S->red_u64[q] = 0ull;
+    if (dt > 0) S->dt = dt;
+  }
 }
 
 int afid_box_reset(afid_ctx *c, int id, double dt) {
@@ -1194,10 +1212,12 @@ int afid_box_reset(afid_ctx *c, int id, double dt) {
   if (rc) return rc;
   const BoxDev &d = hb->dev;
   cudaStream_t st = c->stream;
-  CK(cudaMemsetAsync(d.rux, 0, 4 * (size_t)d.fsize * sizeof(double), st));
-  CK(cudaMemsetAsync(d.wall, 0, (size_t)d.plane * sizeof(double), st));
-  // the record on the device, in stream order (no host round trip)
-  k_reset_scalars<<<1, 1, 0, st>>>(d.sc, dt);
+  // the RK history and wall row zeroed and the record reset by one kernel
+  // in stream order: no host round trip, and no memset, which may queue on a
+  // copy engine behind other streams' transfers
+  const long long nh = 4 * d.fsize, nw = d.plane;
+  k_reset_box<<<(unsigned)std::min<long long>(cdiv(nh + nw, 256), 4096), 256, 0, st>>>(d.rux, nh, d.wall, nw,
+                                                                                       d.sc, dt);
   CKL();
   return 0;
 }
@@ -1380,6 +1400,19 @@ int afid_boxes_get_scalars_async(afid_ctx *c, const int *ids, int n, afid_box_sc
   // the stream's staging array serves every call on it: each call's copy is
   // queued right behind its gather, and the next call's gather behind that
   // copy, so no record is overwritten before it is copied
+  // pinned host memory the device can reach: the gather writes the records
+  // there itself, so the read puts no copy on a copy engine (where it could
+  // wait behind other streams' transfers)
+  {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer) {
+      k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n,
+                                                                     (afid_box_scalars *)pa.devicePointer);
+      CKL();
+      return 0;
+    }
+    cudaGetLastError();   // pageable memory: not an error
+  }
   const size_t need = (sizeof(afid_box_scalars) * n + sizeof(BoxScalars) - 1) / sizeof(BoxScalars);
   afid_ctx::RecStage *rs;
   rc = rec_stage(c, (int)need, false, &rs);
@@ -1782,7 +1815,7 @@ int afid_step_graph(afid_ctx *c, const int *ids, int n, int nsteps) {
   Batch *bt;
   rc = get_batch(c, ids, n, &bt);
   if (rc) return rc;
-  if (bt->split) {
+  if (bt->split && c->split_sets) {
     // each half steps on its own stream between a fork from and a join to
     // the context's stream; the halves are independent, so they need no
     // other ordering
@@ -1812,7 +1845,7 @@ int afid_step_graph_kernels(afid_ctx *c, const int *ids, int n, int *kernels) {
   Batch *bt;
   rc = get_batch(c, ids, n, &bt);
   if (rc) return rc;
-  if (bt->split) {
+  if (bt->split && c->split_sets) {
     Batch *hb[2];
     rc = split_halves(c, bt, hb);
     if (rc) return rc;

@@ -90,6 +90,11 @@ class Context:
     def set_stream(self, handle: int | None):
         _lib.check(self._L.afid_ctx_set_stream(self.h, C.c_void_p(handle or 0)))
 
+    def set_split_sets(self, on: bool):
+        """Run large box sets as two halves on two streams in graph steps
+        (the default) or whole (see afid_ctx_set_split_sets)."""
+        _lib.check(self._L.afid_ctx_set_split_sets(self.h, 1 if on else 0))
+
     def synchronize(self):
         _lib.check(self._L.afid_ctx_synchronize(self.h))
 

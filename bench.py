@@ -53,6 +53,11 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# Streams share the device's hardware work queues (8 by default); two streams
+# on one queue run in issue order.  The end-to-end leg runs two halves of the
+# boxes on two streams, and a split set's halves run on two more, so ask for
+# the maximum before CUDA starts (a setting of this process only).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC_BATCH = "Mpoint-steps/s FP64 (batched/served vs plain, same B200); p50/p99 solve latency"
 METRIC_BOX = "Mpoint-steps/s FP64 (RK3 step, cells = nxm*nym*nzm)"
@@ -459,14 +464,19 @@ def roofline_of(ctx, boxes, cfgs, prof_steps=2, ensemble=False):
 
 
 def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
-    """The same steps through the public C-ABI from pinned host buffers:
-    upload of the initial fields (queued), per step afid_step_graph + every
-    box's result record copied back into that step's slot of a pinned buffer
-    (afid_boxes_get_scalars_async), download of the final fields (queued),
-    one wait at the end."""
+    """The same steps through the public C-ABI from pinned host buffers, the
+    boxes in two halves of about equal cells, each half on its own stream
+    (afid_ctx_set_stream) with the context's own set splitting off: upload
+    of the half's initial fields (queued; the second half's behind the
+    first's), reset, per step afid_step_graph + every box's result record of
+    that step (afid_boxes_get_scalars_async, written by the device into that
+    step's slot of a pinned buffer), download of the final fields (queued);
+    one wait at the end.  One half's copies overlap the other half's
+    steps."""
     import ctypes as C
     torch = D.torch
     from afid_b200 import _lib
+    from afid_b200.ensemble import shard
     from afid_b200.ic import initial_fields
     L = _lib.lib()
     fields = ["vx", "vy", "vz", "temp", "pr"]
@@ -479,45 +489,94 @@ def e2e_run(ctx, boxes, cfgs, seeds, nsteps, D: Dist):
             t_in.numpy()[...] = f[k].transpose(2, 1, 0)
             ins[k] = t_in          # the final fields overwrite the initial ones
         host.append(ins)
-    ids = (C.c_int * len(boxes))(*[b.id for b in boxes])
-    sc = _lib.BoxScalars()   # size of one per-box record read back per step
+    parts = [p for p in (shard(cfgs, r, 2) for r in range(2)) if p] if len(boxes) > 1 else [[0]]
+    ids = [(C.c_int * len(p))(*[boxes[q].id for q in p]) for p in parts]
+    streams = [torch.cuda.Stream(device=D.local) for _ in parts]
+    rec_size = C.sizeof(_lib.BoxScalars)
     h2d = sum(5 * cfg.nx * cfg.nym * cfg.nzm * 8 for cfg in cfgs)
+    nb = len(boxes)
+    # one pinned slot of records per step and part, read on the host after
+    # the final wait
+    rec_buf = torch.empty(nsteps * nb * rec_size, dtype=torch.uint8, pin_memory=True)
+    recs = (_lib.BoxScalars * (nsteps * nb)).from_address(rec_buf.data_ptr())
+    own = ctx.stream
+    ctx.set_split_sets(False)
+    for h, p in enumerate(parts):      # each part's graph on its stream, outside the timing
+        ctx.set_stream(streams[h].cuda_stream)
+        _lib.check(L.afid_step_graph(ctx.h, ids[h], len(p), 0))
     torch.cuda.synchronize()
     D.barrier()
-    # one pinned slot of records per step: each step's records are copied back
-    # behind that step, and read on the host after the final wait
-    nb = len(boxes)
-    rec_buf = torch.empty(nsteps * nb * C.sizeof(_lib.BoxScalars), dtype=torch.uint8, pin_memory=True)
-    recs = (_lib.BoxScalars * (nsteps * nb)).from_address(rec_buf.data_ptr())
+    marks = {}
+
+    def mark(name, st):                # device timeline of the leg
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(st)
+        marks[name] = e
     t0 = time.perf_counter()
-    for b, ins in zip(boxes, host):     # queued: the copies run back to back on the stream
-        for k in fields:
-            _lib.check(L.afid_box_upload_async(ctx.h, b.id, _lib.FIELDS[k],
-                                               C.cast(ins[k].data_ptr(), C.POINTER(C.c_double))))
-    for b in boxes:
-        _lib.check(L.afid_box_reset(ctx.h, b.id, 0.0))
-    for s in range(nsteps):
-        _lib.check(L.afid_step_graph(ctx.h, ids, nb, 1))
-        slot = C.cast(C.addressof(recs) + s * nb * C.sizeof(_lib.BoxScalars), C.POINTER(_lib.BoxScalars))
-        _lib.check(L.afid_boxes_get_scalars_async(ctx.h, ids, nb, slot))
-    for b, outs in zip(boxes, host):
-        for k in fields:
-            _lib.check(L.afid_box_download_async(ctx.h, b.id, _lib.FIELDS[k],
-                                                 C.cast(outs[k].data_ptr(), C.POINTER(C.c_double))))
-    _lib.check(L.afid_ctx_synchronize(ctx.h))
-    t3 = time.perf_counter()
-    t = D.max(t3 - t0)
+    mark("start", streams[0])
+    for st in streams[1:]:
+        st.wait_event(marks["start"])
+    uploaded = None
+    for h, p in enumerate(parts):      # queued; part h + 1's copies wait for part h's
+        ctx.set_stream(streams[h].cuda_stream)
+        if uploaded is not None:
+            streams[h].wait_event(uploaded)
+        for q in p:
+            for k in fields:
+                _lib.check(L.afid_box_upload_async(ctx.h, boxes[q].id, _lib.FIELDS[k],
+                                                   C.cast(host[q][k].data_ptr(), C.POINTER(C.c_double))))
+        uploaded = torch.cuda.Event()
+        uploaded.record(streams[h])
+        mark(f"uploaded{h}", streams[h])
+    bases = [sum(len(x) for x in parts[:h]) for h in range(len(parts))]
+    for h, p in enumerate(parts):
+        ctx.set_stream(streams[h].cuda_stream)
+        for q in p:
+            _lib.check(L.afid_box_reset(ctx.h, boxes[q].id, 0.0))
+    # the parts' steps issued in turn, step by step, part h offset by `lead`
+    # steps per part before it (part 0 steps while part 1's data is still
+    # coming in; part 0's downloads go out while part 1 finishes); streams
+    # that share a hardware queue then alternate instead of running one part
+    # after the other
+    lead = min(3, nsteps)
+    order = sorted(((s + h * lead, h, s) for h in range(len(parts)) for s in range(nsteps)))
+    done = [0] * len(parts)
+
+    def downloads(h):
+        ctx.set_stream(streams[h].cuda_stream)
+        mark(f"stepped{h}", streams[h])
+        for q in parts[h]:
+            for k in fields:
+                _lib.check(L.afid_box_download_async(ctx.h, boxes[q].id, _lib.FIELDS[k],
+                                                     C.cast(host[q][k].data_ptr(), C.POINTER(C.c_double))))
+        mark(f"downloaded{h}", streams[h])
+    for _, h, s in order:
+        p = parts[h]
+        ctx.set_stream(streams[h].cuda_stream)
+        _lib.check(L.afid_step_graph(ctx.h, ids[h], len(p), 1))
+        slot = C.cast(C.addressof(recs) + (s * nb + bases[h]) * rec_size, C.POINTER(_lib.BoxScalars))
+        _lib.check(L.afid_boxes_get_scalars_async(ctx.h, ids[h], len(p), slot))
+        done[h] += 1
+        if done[h] == nsteps:
+            downloads(h)
+    for st in streams:
+        st.synchronize()
+    t = D.max(time.perf_counter() - t0)
+    ctx.set_stream(own)
+    ctx.set_split_sets(True)
     if any(recs[(nsteps - 1) * nb + q].status != 0 for q in range(nb)) or \
             any(recs[s * nb].ntime != recs[0].ntime + s for s in range(nsteps)):
         raise RuntimeError("e2e: a box stopped with a status code, or a record is missing")
     ncell = D.sum(sum(cells(c) for c in cfgs))
     return {"value": ncell * nsteps / t / 1e6, "unit": UNIT,
             "h2d_bytes_per_step": D.sum(h2d) / nsteps,
-            "d2h_bytes_per_step": D.sum(h2d + C.sizeof(sc) * nsteps * len(boxes)) / nsteps,
-            "what": "afid_box_upload_async of the initial fields from pinned host memory, K x "
-                    "(afid_step_graph + afid_boxes_get_scalars_async: every box's record of that step "
-                    "copied to pinned host memory), afid_box_download_async of the final fields, "
-                    "afid_ctx_synchronize"}
+            "d2h_bytes_per_step": D.sum(h2d + rec_size * nsteps * nb) / nsteps,
+            "parts": len(parts),
+            "timeline_ms": {k: round(marks["start"].elapsed_time(e), 2) for k, e in marks.items() if k != "start"},
+            "what": "boxes in two halves, each on its own stream: afid_box_upload_async of the initial "
+                    "fields from pinned host memory, afid_box_reset, K x (afid_step_graph + "
+                    "afid_boxes_get_scalars_async: every box's record of that step into pinned host "
+                    "memory), afid_box_download_async of the final fields; one wait"}
 
 
 def serve_record(ctx, D: Dist, rate: float, nreq: int, steps: int, quantum: int = 32) -> dict:

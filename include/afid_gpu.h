@@ -113,6 +113,12 @@ int afid_ctx_destroy(afid_ctx *ctx);
 int afid_ctx_set_stream(afid_ctx *ctx, void *stream);
 void *afid_ctx_stream(afid_ctx *ctx);
 int afid_ctx_synchronize(afid_ctx *ctx);
+/* Whether afid_step_graph runs large sets as two halves on two streams of
+ * the context (1, the default; AFID_BATCH_STREAMS=1 in the environment makes
+ * 0 the default) or whole (0).  A caller that splits its boxes itself, one
+ * stream per part, turns it off so that its parts do not share the
+ * context's two streams (no counterpart in the reference). */
+int afid_ctx_set_split_sets(afid_ctx *ctx, int on);
 
 /* ---- grid and boxes ------------------------------------------------------
  * afid_make_grid: node positions xc(1..nx) of CreateGrid.F90:66-119 for
@@ -167,7 +173,8 @@ int afid_boxes_get_scalars(afid_ctx *ctx, const int *box_ids, int n, afid_box_sc
 /* The same records queued on the context's stream, returning at once (no
  * counterpart in the reference): out[0..n) is filled once the stream gets
  * there (after afid_ctx_synchronize at the latest) and must stay valid
- * until then; from pinned host memory the copy overlaps later queued work.
+ * until then.  Into pinned host memory the records are written by the
+ * device directly (no copy); other memory is filled by a queued copy.
  * Each call's records are those of the boxes at that point of the stream. */
 int afid_boxes_get_scalars_async(afid_ctx *ctx, const int *box_ids, int n, afid_box_scalars *out);
 /* Hold points of a box (no counterpart in the reference; they move the
@@ -232,8 +239,8 @@ int afid_calc_plate_nu(afid_ctx *ctx, int box_id, double *nuslow, double *nusupp
  * CUDA graph of one step, captured on first use per box set.  A set of at
  * least 8 boxes and 4 Mi cells runs there as two halves of about equal
  * cells, each with its own graph on a stream of the context, forked from
- * and joined back to the context's stream (AFID_BATCH_STREAMS=1 in the
- * environment keeps sets whole); the results are the same either way. */
+ * and joined back to the context's stream (afid_ctx_set_split_sets); the
+ * results are the same either way. */
 int afid_step(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
 int afid_step_graph(afid_ctx *ctx, const int *box_ids, int nbox, int nsteps);
 /* Kernels one afid_step_graph step of this set launches (both halves of a

@@ -210,8 +210,9 @@ def test_split_graph_equals_direct(ctx):
 def test_queued_records_on_two_streams(ctx):
     """Two box sets stepped and read back on two streams of one context,
     queued one after the other with no wait between: each stream's records
-    are its own set's (the record staging is per stream), and a queued
-    reset takes effect in stream order."""
+    are its own set's (pageable memory through a per-stream staging array,
+    pinned memory written directly), and a queued reset takes effect in
+    stream order."""
     import ctypes as C
 
     import torch
@@ -221,7 +222,10 @@ def test_queued_records_on_two_streams(ctx):
     sets = [[_add(ctx, kw, 70 + 10 * h + q) for q, kw in enumerate(MIX[:2])] for h in range(2)]
     streams = [torch.cuda.Stream() for _ in sets]
     own = ctx.stream
-    slots = [(_lib.BoxScalars * 2)() for _ in sets]
+    # stream 0 reads into pageable memory (a queued copy through the stream's
+    # staging), stream 1 into pinned memory (written by the device itself)
+    pinned = torch.empty(2 * C.sizeof(_lib.BoxScalars), dtype=torch.uint8, pin_memory=True)
+    slots = [(_lib.BoxScalars * 2)(), (_lib.BoxScalars * 2).from_address(pinned.data_ptr())]
     try:
         for h, (boxes, st) in enumerate(zip(sets, streams)):
             ctx.set_stream(st.cuda_stream)
