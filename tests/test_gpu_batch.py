@@ -202,7 +202,17 @@ def test_split_graph_equals_direct(ctx):
             assert np.array_equal(g.download(f), d.download(f)), f
         assert g.scalars() == d.scalars()
     one = ctx.graph_kernels(graphed[:1])
-    assert ctx.graph_kernels(graphed) > one
+    split = ctx.graph_kernels(graphed)
+    assert split > one
+    ctx.set_split_sets(False)     # the whole set in one graph: one launch per stage
+    try:
+        assert ctx.graph_kernels(graphed) == one
+        ctx.step(graphed, 1, graph=True)
+        ctx.step(direct, 1)
+        for g, d in zip(graphed, direct):
+            assert np.array_equal(g.download("temp"), d.download("temp"))
+    finally:
+        ctx.set_split_sets(True)
     for b in graphed + direct:
         ctx.remove_box(b)
 
