@@ -511,6 +511,18 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out, bool allow_split 
     devs.push_back(d);
     fft_smem_grow(d, bt->sm_y, bt->sm_z, twy_max, twz_max);
   }
+  // Boxes of more planes first: a block of a column march (or of the
+  // explicit kernel's tiles) takes time in proportion to its box's nxm, and
+  // with the longest blocks started first the short ones fill the end of the
+  // launch.  pos[b] is the caller's position of the batch's box b.
+  std::vector<int> pos(n), bids(n);
+  for (int b = 0; b < n; ++b) pos[b] = b;
+  std::stable_sort(pos.begin(), pos.end(), [&](int a, int b) { return devs[a].nxm > devs[b].nxm; });
+  {
+    std::vector<BoxDev> sorted(n);
+    for (int b = 0; b < n; ++b) { sorted[b] = devs[pos[b]]; bids[b] = ids[pos[b]]; }
+    devs.swap(sorted);
+  }
   bt->smem_y = (size_t)(2 * bt->sm_y.slot + twy_max) * 16 + FFT_TAIL_BYTES;   // + mbarriers, descriptor
   bt->smem_z = (size_t)(2 * bt->sm_z.slot + twz_max) * 16 + FFT_TAIL_BYTES;
   {
@@ -538,6 +550,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out, bool allow_split 
     off[(size_t)f * (n + 1) + n] = (int)acc;
     bt->total[f] = (int)acc;
   }
+  off.insert(off.end(), pos.begin(), pos.end());   // the positions follow the tile tables
   if (cudaMalloc(&bt->d_boxes, sizeof(BoxDev) * n) != cudaSuccess ||
       cudaMalloc(&bt->d_off, sizeof(int) * off.size()) != cudaSuccess) {
     free_batch(bt);
@@ -569,7 +582,7 @@ int get_batch(afid_ctx *c, const int *ids, int n, Batch **out, bool allow_split 
         side[b] = h;
         load[h] += (long long)devs[b].nxm * devs[b].plane;
       }
-      for (int b = 0; b < n; ++b) bt->half_ids[side[b]].push_back(ids[b]);
+      for (int b = 0; b < n; ++b) bt->half_ids[side[b]].push_back(bids[b]);
       bt->split = !bt->half_ids[0].empty() && !bt->half_ids[1].empty();
     }
   }
@@ -648,6 +661,9 @@ int launch_fft_y(bool fwd, const int *total, BD bd, int grid_y, size_t smem_y, F
   }
   return 0;
 }
+
+// the caller's positions of the batch's boxes (after the tile tables)
+const int *batch_pos(const Batch *bt) { return bt->d_off + (size_t)NFAM * (bt->ids.size() + 1); }
 
 BatchDev bdev(const Batch *bt, int fam) {
   BatchDev d;
@@ -1355,13 +1371,13 @@ static void scalars_out(const BoxScalars &bs, afid_box_scalars *out) {
   out->nu_bot = bs.nu_bot; out->nu_top = bs.nu_top; out->ntime = bs.ntime; out->status = bs.status;
 }
 
-__global__ void k_gather_scalars(const BoxDev *boxes, int n, BoxScalars *dst) {
+__global__ void k_gather_scalars(const BoxDev *boxes, const int *pos, int n, BoxScalars *dst) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < n) dst[b] = *boxes[b].sc;
+  if (b < n) dst[pos[b]] = *boxes[b].sc;
 }
 
 // the public records of n boxes, written straight in afid_box_scalars layout
-__global__ void k_gather_records(const BoxDev *boxes, int n, afid_box_scalars *dst) {
+__global__ void k_gather_records(const BoxDev *boxes, const int *pos, int n, afid_box_scalars *dst) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   const BoxScalars &bs = *boxes[b].sc;
@@ -1369,7 +1385,7 @@ __global__ void k_gather_records(const BoxDev *boxes, int n, afid_box_scalars *d
   o.dt = bs.dt; o.time = bs.time; o.cfl = bs.cfl; o.cfl_used = bs.cfl_used; o.divmax = bs.divmax;
   for (int q = 0; q < 3; ++q) o.vmax[q] = bs.vmax[q];
   o.nu_bot = bs.nu_bot; o.nu_top = bs.nu_top; o.ntime = bs.ntime; o.status = bs.status;
-  dst[b] = o;
+  dst[pos[b]] = o;
 }
 
 int afid_boxes_get_scalars(afid_ctx *c, const int *ids, int n, afid_box_scalars *out) {
@@ -1382,7 +1398,7 @@ int afid_boxes_get_scalars(afid_ctx *c, const int *ids, int n, afid_box_scalars 
   afid_ctx::RecStage *rs;
   rc = rec_stage(c, n, true, &rs);
   if (rc) return rc;
-  k_gather_scalars<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, rs->d);
+  k_gather_scalars<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, batch_pos(bt), n, rs->d);
   CKL();
   CK(cudaMemcpyAsync(rs->h, rs->d, sizeof(BoxScalars) * n, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1406,7 +1422,7 @@ int afid_boxes_get_scalars_async(afid_ctx *c, const int *ids, int n, afid_box_sc
   {
     cudaPointerAttributes pa;
     if (cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer) {
-      k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n,
+      k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, batch_pos(bt), n,
                                                                      (afid_box_scalars *)pa.devicePointer);
       CKL();
       return 0;
@@ -1418,7 +1434,7 @@ int afid_boxes_get_scalars_async(afid_ctx *c, const int *ids, int n, afid_box_sc
   rc = rec_stage(c, (int)need, false, &rs);
   if (rc) return rc;
   afid_box_scalars *d = reinterpret_cast<afid_box_scalars *>(rs->d);
-  k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, n, d);
+  k_gather_records<<<(unsigned)cdiv(n, 128), 128, 0, c->stream>>>(bt->d_boxes, batch_pos(bt), n, d);
   CKL();
   CK(cudaMemcpyAsync(out, d, sizeof(afid_box_scalars) * n, cudaMemcpyDeviceToHost, c->stream));
   return 0;
