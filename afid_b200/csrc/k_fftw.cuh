@@ -51,6 +51,23 @@ __host__ __device__ constexpr int wf_warps(int V) { return V == 12 ? 6 : 8; }
 // (N/2 + 1) values) for the inverse; with G >= 2 lanes per line (LPW <= 16)
 // both fit in 32 V + 32.
 __host__ __device__ constexpr int wf_buf(int V) { return 32 * V + 32; }
+
+// Index of line l's value n in a warp buffer: n LPW + l, plus one complex of
+// pad per 8 values of n.  Without the pad, a radix-8 pass writes the eight
+// values of each lane's butterfly 8 rows (8 LPW complex) apart, which for
+// LPW = 4 is 512 bytes: the same banks for all lanes.  N LPW + N / 8 <= 32 V
+// + 16 fits the buffer.
+__device__ __forceinline__ int wsidx(int l, int n, int lgL) { return (n << lgL) + l + (n >> 3); }
+struct WSmemDst {
+  double2 *a;
+  int lgL;
+  __device__ __forceinline__ void operator()(int l, int n, double2 v) const { a[wsidx(l, n, lgL)] = v; }
+};
+struct WSmemSrc {
+  const double2 *a;
+  int lgL;
+  __device__ __forceinline__ double2 operator()(int l, int n) const { return a[wsidx(l, n, lgL)]; }
+};
 // A warp's slice: twiddles (WF_MAX_N complex), radices (8 ints, 32 bytes),
 // then the two buffers.
 __host__ __device__ constexpr int wf_slice(int V) { return WF_MAX_N + 2 + 2 * wf_buf(V); }
@@ -160,8 +177,8 @@ __device__ __forceinline__ void wrun(int R, int N, int lgL, int Ns, const double
 template <int SGN, int V, class Src, class Dst>
 __device__ __forceinline__ void wfft(double2 *a, int N, int lgL, const int *rad, int np, const double2 *tw,
                                      const Src &src, const Dst &dst) {
-  const SmemSrc as{a, lgL};
-  const SmemDst ad{a, lgL};
+  const WSmemSrc as{a, lgL};
+  const WSmemDst ad{a, lgL};
   if (np == 1) {
     wrun<SGN, V>(rad[0], N, lgL, 1, tw, src, dst);
     return;
@@ -234,7 +251,7 @@ enum { WK_YF = 0, WK_YI = 1, WK_Z = 2 };
 //          the shared-memory banks);
 //   WK_YI: the unit's 2 LPW half-spectrum rows, contiguous in HBM;
 //   WK_Z:  the unit's LPW columns, kz row by kz row (LPW consecutive values
-//          of each row), to a[n LPW + l], the layout of the passes.
+//          of each row), to a[wsidx(l, n)], the layout of the passes.
 template <int KIND, bool ZD>
 __device__ __forceinline__ void wf_issue(const WarpBox<ZD> &P, int lu, double2 *a) {
   const int lane = threadIdx.x & 31;
@@ -245,8 +262,9 @@ __device__ __forceinline__ void wf_issue(const WarpBox<ZD> &P, int lu, double2 *
     const int ne = P.N << P.lgL, lmask = P.lpw - 1;
     for (int e = lane; e < ne; e += 32) {
       const int n = e >> P.lgL, l = e & lmask;
-      if (ky0 + l < P.nh) cp_async16(a + e, S + (long long)n * P.nh + l);
-      else a[e] = zero;
+      double2 *d = a + wsidx(l, n, P.lgL);
+      if (ky0 + l < P.nh) cp_async16(d, S + (long long)n * P.nh + l);
+      else *d = zero;
     }
   } else {
     const int k = lu / P.upp, i0 = (lu - k * P.upp) * 2 * P.lpw;
@@ -281,13 +299,13 @@ __device__ __forceinline__ void wf_process(const WarpBox<ZD> &X, int lu, double2
   if constexpr (KIND == WK_Z) {
     const int k = lu / X.upp, ky0 = (lu - k * X.upp) * lpw;
     double2 *const S = X.spec + (long long)k * X.nzm * nh;
-    wfft<SGN, V>(a, N, lgL, rad, X.np, tws, SmemSrc{a, lgL}, WColDst{S, nh, ky0});
+    wfft<SGN, V>(a, N, lgL, rad, X.np, tws, WSmemSrc{a, lgL}, WColDst{S, nh, ky0});
   } else {
     const int k = lu / X.upp, i0 = (lu - k * X.upp) * 2 * lpw;
     const int nrow = min(2 * lpw, X.nzm - i0);
     if constexpr (KIND == WK_YF) {
       wfft<-1, V>(a, N, lgL, rad, X.np, tws, WStagedRowPairSrc{reinterpret_cast<const double *>(a), N + 2},
-                  SmemDst{a, lgL});
+                  WSmemDst{a, lgL});
       // unpack the two real transforms of line l: A = (Z_q + conj Z_{N-q}) / 2,
       // B = (Z_q - conj Z_{N-q}) / (2i), q <= N/2
       const int lane = threadIdx.x & 31;
@@ -295,8 +313,8 @@ __device__ __forceinline__ void wf_process(const WarpBox<ZD> &X, int lu, double2
       double2 *const speck = X.spec + (long long)k * X.nzm * nh;
       const int i = i0 + 2 * l;
       for (int q = lane >> lgL; q < nh; q += g) {
-        const double2 z = a[sidx(l, q, lgL)];
-        const double2 zn = a[sidx(l, q == 0 ? 0 : N - q, lgL)];
+        const double2 z = a[wsidx(l, q, lgL)];
+        const double2 zn = a[wsidx(l, q == 0 ? 0 : N - q, lgL)];
         const double2 A = make_double2((z.x + zn.x) * 0.5, (z.y - zn.y) * 0.5);
         const double2 Bv = make_double2((z.y + zn.y) * 0.5, (zn.x - z.x) * 0.5);
         if (i < X.nzm) __stcg(speck + (long long)i * nh + q, A);
